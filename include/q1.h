@@ -1,0 +1,352 @@
+/*
+ * q1.h -- C ABI of the B200-native TPC-H Query 1 filter + group-by aggregation path.
+ *
+ * Every entry point is plain C: integers, pointers and sizes; no C++ or torch types.
+ * Every call returns a q1_status; nothing throws across this boundary.
+ *
+ * Each declaration names the reference interface it replaces (paths are relative to
+ * the diegomestre2/tpchQ01_GPU source tree).
+ *
+ * Fixed-point conventions (identical to the reference CPU kernels, cpu/kernel_hyper.hpp:18-64):
+ *   quantity, discount, tax      Decimal(15,2): hundredths          (cpu/tpch_kit.hpp:42-83)
+ *   extendedprice                cents (hundredths)
+ *   disc_price = (100 - d) * p   scale 1e-4
+ *   charge = disc_price*(100+t)  scale 1e-6
+ *   shipdate                     MonetDB day number (cpu/monetdb.cpp:62-78); 727563 = 1992-01-01
+ * All sums are exact two's-complement 128-bit integers.
+ */
+#ifndef Q1_H_
+#define Q1_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------ */
+/* Status codes                                                                                 */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef enum q1_status {
+    Q1_OK                   = 0,
+    Q1_ERR_INVALID_ARGUMENT = 1,  /* bad parameter combination (src/main.cu:255-360 validation) */
+    Q1_ERR_CUDA             = 2,  /* a CUDA runtime call failed; see q1_last_error()            */
+    Q1_ERR_OUT_OF_MEMORY    = 3,  /* device or pinned allocation failed                          */
+    Q1_ERR_NOT_LOADED       = 4,  /* q1_run before q1_load_columns                              */
+    Q1_ERR_UNSUPPORTED      = 5,  /* layout / placement combination not offered                 */
+    Q1_ERR_DOMAIN           = 6,  /* a value does not fit the compressed column types          */
+    Q1_ERR_DEVICE_TIMEOUT   = 7,  /* a bounded device-side wait expired; the context stays usable */
+    Q1_ERR_BUSY             = 8,  /* serving: admission refused (slots or memory budget)         */
+    Q1_ERR_CPU_WORKER       = 9,  /* a coprocessing CPU worker failed                            */
+    Q1_ERR_INTERNAL         = 10
+} q1_status;
+
+/* Human-readable text of the last error raised on the calling thread (never NULL). */
+const char* q1_last_error(void);
+/* Name of a status code. */
+const char* q1_status_string(q1_status s);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Constants                                                                                    */
+/* ------------------------------------------------------------------------------------------ */
+
+enum {
+    Q1_NUM_POTENTIAL_GROUPS   = 6,       /* 3 return flags x 2 line stati (src/constants.hpp:56) */
+    Q1_NUM_AGGREGATES         = 6,       /* count, qty, base_price, disc, disc_price, charge     */
+    Q1_SHIP_DATE_FRAME        = 727563,  /* 1992-01-01 (src/constants.hpp:50)                   */
+    Q1_DEFAULT_CUTOFF_DAY     = 729999,  /* 1998-12-01 minus 90 days (cpu/common.cpp:60)        */
+    Q1_MAX_KEY_GROUPS         = 65536    /* group-key aggregation (synthetic uint32 key)          */
+};
+
+/* Order of the six aggregates inside one group's record of the device aggregate buffer. */
+typedef enum q1_aggregate {
+    Q1_AGG_COUNT          = 0,
+    Q1_AGG_SUM_QTY        = 1,  /* hundredths                */
+    Q1_AGG_SUM_BASE_PRICE = 2,  /* cents                     */
+    Q1_AGG_SUM_DISC       = 3,  /* hundredths, sum of d      */
+    Q1_AGG_SUM_DISC_PRICE = 4,  /* 1e-4                      */
+    Q1_AGG_SUM_CHARGE     = 5   /* 1e-6                      */
+} q1_aggregate;
+
+/* Hash-table placements of src/main.cu:166-191 (README spelling in comments). */
+typedef enum q1_placement {
+    Q1_PLACEMENT_IN_REGISTERS            = 0, /* "in-registers": warp-lane tables (ht_in_registers.cuh)   */
+    Q1_PLACEMENT_IN_REGISTERS_PER_THREAD = 1, /* default (ht_in_registers_per_thread.cuh)                  */
+    Q1_PLACEMENT_LOCAL_MEM               = 2, /* "local-mem" (ht_in_local_mem.cuh)                          */
+    Q1_PLACEMENT_SHARED_MEM_PER_THREAD   = 3, /* "per-thread-shared-mem" (ht_in_shared_mem_per_thread.cuh) */
+    Q1_PLACEMENT_GLOBAL                  = 4, /* "global" (ht_in_global_mem.hpp)                           */
+    Q1_NUM_PLACEMENTS                    = 5
+} q1_placement;
+
+/* Parse a placement name; accepts both the code spelling (in_registers_per_thread, local_mem,
+ * shared_mem_per_thread, ...) and the README spelling (in-registers, local-mem,
+ * per-thread-shared-mem, ...). Returns Q1_ERR_INVALID_ARGUMENT for unknown names. */
+q1_status q1_placement_from_name(const char* name, q1_placement* out);
+const char* q1_placement_name(q1_placement p);
+
+typedef enum q1_layout {
+    Q1_LAYOUT_UNCOMPRESSED = 0,  /* reference-typed columns, 38 B/row (src/data_types.h:19-25)        */
+    Q1_LAYOUT_COMPRESSED   = 1   /* uint16 day offset, uint8 qty/disc/tax, uint32 cents, packed flags */
+} q1_layout;
+
+typedef enum q1_flag_packing {
+    Q1_FLAGS_PAIR_2BIT = 0,      /* (returnflag, linestatus) pair dictionary, 2 bits/row: 9.25 B/row   */
+    Q1_FLAGS_SEPARATE  = 1       /* returnflag 2 bits + linestatus 1 bit (src/main.cu:787-790): 9.375  */
+} q1_flag_packing;
+
+typedef enum q1_residency {
+    Q1_RESIDENCY_HBM         = 0, /* columns copied once into device memory                         */
+    Q1_RESIDENCY_PINNED_HOST = 1  /* columns stay in pinned host memory; every run streams them      */
+} q1_residency;
+
+/* ------------------------------------------------------------------------------------------ */
+/* Column sets                                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Uncompressed lineitem columns with the reference's element types (src/data_types.h:19-25,
+ * cpu/tpch_kit.hpp:135-149). Host or device pointers depending on the call. */
+typedef struct q1_columns {
+    const int32_t* shipdate;       /* MonetDB day number      */
+    const int64_t* discount;       /* hundredths              */
+    const int64_t* extendedprice;  /* cents                   */
+    const int64_t* tax;            /* hundredths              */
+    const int64_t* quantity;       /* hundredths              */
+    const char*    returnflag;     /* 'A' | 'N' | 'R'         */
+    const char*    linestatus;     /* 'F' | 'O'               */
+} q1_columns;
+
+/* Compressed columns (src/main.cu:773-803, namespace compressed in src/data_types.h:37-44).
+ * Bit containers are uint32 words, element i at word i/(32/b), bit b*(i%(32/b)), LSB first
+ * (src/bit_operations.hpp:60-154). */
+typedef struct q1_compressed_columns {
+    const uint16_t* shipdate;      /* day - 727563                                              */
+    const uint8_t*  discount;      /* hundredths, 0..100                                        */
+    const uint32_t* extendedprice; /* cents                                                     */
+    const uint8_t*  tax;           /* hundredths                                                */
+    const uint8_t*  quantity;      /* whole units (reference divides by 100, src/main.cu:783)   */
+    const uint32_t* flags;         /* Q1_FLAGS_PAIR_2BIT: 2-bit pair codes                      */
+    const uint32_t* returnflag;    /* Q1_FLAGS_SEPARATE: 2-bit codes A=0 N=1 R=2               */
+    const uint32_t* linestatus;    /* Q1_FLAGS_SEPARATE: 1-bit codes F=0 O=1                   */
+    const uint32_t* filter;        /* optional precomputed predicate bitmap, 1 bit/row          */
+    int32_t         flag_packing;  /* q1_flag_packing                                           */
+    uint32_t        num_pair_codes;/* PAIR_2BIT: number of dictionary entries (1..4)            */
+    uint8_t         pair_group[4]; /* PAIR_2BIT: code -> group index (rf_code<<1 | ls_code)     */
+} q1_compressed_columns;
+
+/* Column statistics produced by the compressor (the analogue of cpu/tpch_kit.hpp:95-108 MinMax). */
+typedef struct q1_column_stats {
+    uint64_t rows;
+    int32_t  min_shipdate, max_shipdate;
+    uint32_t max_quantity, max_discount, max_tax;
+    uint32_t max_extendedprice;
+    uint32_t num_pair_codes;
+    uint8_t  pair_group[4];
+    uint32_t group_present_mask;   /* bit g set if group g occurs */
+} q1_column_stats;
+
+/* Host-side compressor: reference-typed columns -> compressed columns (src/main.cu:773-803).
+ * Output buffers are caller-owned host memory: shipdate[rows], discount[rows], tax[rows],
+ * quantity[rows], extendedprice[rows]; for PAIR_2BIT flags[ceil(rows/16)];
+ * for SEPARATE returnflag[ceil(rows/16)] and linestatus[ceil(rows/32)].
+ * Fails with Q1_ERR_DOMAIN if a value does not fit (the reference asserts at :789-800);
+ * in addition discount must be <= 100 and quantity a whole number of units. */
+typedef struct q1_compressed_host_out {
+    uint16_t* shipdate;
+    uint8_t*  discount;
+    uint32_t* extendedprice;
+    uint8_t*  tax;
+    uint8_t*  quantity;
+    uint32_t* flags;
+    uint32_t* returnflag;
+    uint32_t* linestatus;
+} q1_compressed_host_out;
+
+q1_status q1_compress_host(const q1_columns* in, uint64_t rows, q1_flag_packing packing,
+                           const q1_compressed_host_out* out, q1_column_stats* stats);
+
+/* Filter precomputation: bitmap[i/32] bit i%32 = (shipdate[i] <= cutoff - 727563)
+ * (src/main.cu:362-389). Host version writes ceil(rows/32) words. */
+q1_status q1_precompute_filter_host(const uint16_t* shipdate, uint64_t rows, int32_t cutoff_day,
+                                    uint32_t* bitmap);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Results                                                                                      */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Two's-complement 128-bit integer. */
+typedef struct q1_i128 {
+    uint64_t lo;
+    uint64_t hi;
+} q1_i128;
+
+typedef struct q1_group_result {
+    int32_t  group;            /* rf_code<<1 | ls_code (src/kernels/ht_in_global_mem.hpp:41-42) */
+    char     returnflag;       /* decoded 'A' 'N' 'R'                                          */
+    char     linestatus;       /* decoded 'F' 'O'                                              */
+    uint64_t count;
+    q1_i128  sum_qty;          /* hundredths */
+    q1_i128  sum_base_price;   /* cents      */
+    q1_i128  sum_disc;         /* hundredths */
+    q1_i128  sum_disc_price;   /* 1e-4       */
+    q1_i128  sum_charge;       /* 1e-6       */
+    /* Averages from the exact sums, C integer division (truncation toward zero) as in
+     * Decimal64::GetInt/GetFrac (cpu/tpch_kit.hpp:54-60), each carrying two extra decimals:
+     * avg_qty = sum_qty*100/count (1e-4 units), likewise avg_price and avg_disc. 0 if count==0. */
+    int64_t  avg_qty_e4;
+    int64_t  avg_price_e4;
+    int64_t  avg_disc_e4;
+} q1_group_result;
+
+typedef struct q1_result {
+    uint32_t        num_groups;     /* always Q1_NUM_POTENTIAL_GROUPS                  */
+    q1_group_result groups[Q1_NUM_POTENTIAL_GROUPS];
+    uint64_t        rows_total;
+    uint64_t        rows_gpu;       /* rows aggregated on the GPU                      */
+    uint64_t        rows_cpu;       /* rows aggregated by the coprocessing CPU share   */
+    double          ms_last_run;    /* wall-clock of the last run (src/main.cu:893-905) */
+    double          ms_gpu_last_run;/* CUDA-event time of the GPU part of the last run */
+} q1_result;
+
+/* Convert a device aggregate buffer (num_groups records of Q1_NUM_AGGREGATES q1_i128, laid out
+ * [group][aggregate]) into per-group results with averages. */
+q1_status q1_finalize_groups(const q1_i128* aggregates_host, uint32_t num_groups,
+                             q1_group_result* out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Query context: the reference's tpch_01 driver (src/main.cu:738-916) as a library             */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct q1_ctx q1_ctx;
+
+typedef struct q1_device_opts {
+    int32_t device;          /* CUDA device ordinal (the reference always uses the current one) */
+    int32_t cpu_threads;     /* coprocessing pool size; 0 = hardware_concurrency/2 - 1
+                                (cpu/kernel_x100.hpp:535-548 with wo_core0 = true)              */
+} q1_device_opts;
+
+/* Replaces main()'s device setup (src/main.cu:738-878). */
+q1_status q1_open(q1_ctx** ctx, const q1_device_opts* opts);
+q1_status q1_close(q1_ctx* ctx);
+
+/* Load a table. Replaces load_table_columns_from_files + the compression loop + device
+ * allocation (src/main.cu:391-476, :773-878). `layout` selects what the GPU scans:
+ * UNCOMPRESSED keeps the reference-typed columns, COMPRESSED runs q1_compress_host first.
+ * HBM residency copies the columns to device memory once; PINNED_HOST keeps them in pinned
+ * host memory and every run streams them chunk by chunk (src/main.cu:567-719). */
+q1_status q1_load_columns(q1_ctx* ctx, const q1_columns* host_columns, uint64_t rows,
+                          q1_layout layout, q1_flag_packing packing, q1_residency residency);
+
+/* Load already-compressed host columns (e.g. a column cache) without recompressing. */
+q1_status q1_load_compressed(q1_ctx* ctx, const q1_compressed_columns* host_columns,
+                             uint64_t rows, q1_residency residency);
+
+/* Generate `rows` rows of the seeded synthetic lineitem generator into the context, starting at
+ * row index `first_row` (a multiple of 32). Compressed tables are generated on the device: for
+ * HBM residency straight into place, for PINNED_HOST residency chunk by chunk and copied into
+ * pinned host memory. Uncompressed tables are generated on the host and loaded. */
+q1_status q1_generate_table(q1_ctx* ctx, uint64_t seed, uint64_t first_row, uint64_t rows,
+                            q1_layout layout, q1_flag_packing packing, q1_residency residency);
+
+/* Run parameters: mirror of q1_params_t (src/main.cu:205-240). */
+typedef struct q1_params {
+    int32_t placement;            /* q1_placement; --hash-table-placement                        */
+    int32_t apply_compression;    /* --apply-compression: must match the loaded layout          */
+    int32_t use_filter_pushdown;  /* --use-filter-pushdown (requires compression)               */
+    int32_t use_coprocessing;     /* --use-coprocessing                                          */
+    double  cpu_fraction;         /* --cpu-fraction, 0..1 (default 0.5)                          */
+    int32_t streams;              /* --streams (default 4)                                        */
+    int32_t threads_per_block;    /* --threads-per-block, multiple of 32; 0 = tuned default     */
+    int32_t tuples_per_thread;    /* --tuples-per-thread; 0 = tuned default                     */
+    int64_t tuples_per_launch;    /* --tuples-per-kernel-launch (default 1<<21)                 */
+    int32_t runs;                 /* --runs (default 5); q1_run executes this many times        */
+    int32_t cutoff_day;           /* WHERE l_shipdate <= cutoff_day (default 729999)           */
+} q1_params;
+
+/* Fill with the reference defaults (src/constants.hpp:7-40). */
+void q1_params_default(q1_params* p);
+
+/* Validate like parse_command_line (src/main.cu:325-358). */
+q1_status q1_params_validate(const q1_params* p);
+
+/* Device (or, for PINNED_HOST residency, pinned host) column pointers of the loaded table, for
+ * use with the kernel-level calls below. Exactly one of the two views is filled, by layout. */
+q1_status q1_table_columns(q1_ctx* ctx, q1_compressed_columns* compressed, q1_columns* uncompressed,
+                           uint64_t* rows, q1_layout* layout, q1_residency* residency);
+
+/* Column statistics of the loaded table. */
+q1_status q1_table_stats(q1_ctx* ctx, q1_column_stats* stats);
+
+/* Wall-clock and GPU times (ms) of the runs of the last q1_run (src/main.cu:881-905 writes the
+ * wall-clock ones to results.csv). */
+q1_status q1_run_times(q1_ctx* ctx, double* wall_ms, double* gpu_ms, int32_t capacity, int32_t* count);
+
+/* Execute the query `runs` times (src/main.cu:893-905 loop, execute_query_1_once :498-736).
+ * The result of the last run is written to `out`. */
+q1_status q1_run(q1_ctx* ctx, const q1_params* p, q1_result* out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Kernel-level ABI: the reference's __global__ kernels (src/kernels/) launched on caller-owned */
+/* device memory. Aggregates accumulate into a caller-zeroed buffer of                          */
+/* Q1_NUM_POTENTIAL_GROUPS * Q1_NUM_AGGREGATES q1_i128 ([group][aggregate]), just as the         */
+/* reference kernels atomicAdd into caller-zeroed arrays.                                      */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct q1_launch_config {
+    int32_t threads_per_block;   /* 0 = tuned default */
+    int32_t tuples_per_thread;   /* 0 = tuned default */
+    int32_t blocks;              /* 0 = tuned default (multiple of the SM count) */
+} q1_launch_config;
+
+/* Replaces the kernels_compressed / kernels_filter_pushdown tables (src/main.cu:175-191):
+ * K2, K3, K5, K6, K8, K9, K11, K12, K14, K15. `use_filter` reads cols->filter instead of
+ * cols->shipdate. `status_word` (device, may be NULL) receives a nonzero code if a bounded
+ * device wait expired. */
+q1_status q1_launch_compressed(q1_placement placement, const q1_compressed_columns* dev_cols,
+                               uint64_t rows, int32_t cutoff_day, int32_t use_filter,
+                               const q1_launch_config* cfg, q1_i128* dev_aggregates,
+                               void* cuda_stream);
+
+/* Replaces the kernels table (src/main.cu:166-173): K1, K4, K7, K10, K13. */
+q1_status q1_launch_uncompressed(q1_placement placement, const q1_columns* dev_cols,
+                                 uint64_t rows, int32_t cutoff_day,
+                                 const q1_launch_config* cfg, q1_i128* dev_aggregates,
+                                 void* cuda_stream);
+
+/* The kernel-level calls are asynchronous. This synchronises `cuda_stream` and converts the
+ * current device's kernel status word (bounded-wait expiry, out-of-domain rows) into a status
+ * code, clearing it. Replaces the reference's reliance on cuda-api-wrappers exceptions. */
+q1_status q1_sync_check(void* cuda_stream);
+
+/* Device filter precomputation (GPU version of src/main.cu:362-389). */
+q1_status q1_precompute_filter(const uint16_t* dev_shipdate, uint64_t rows, int32_t cutoff_day,
+                               uint32_t* dev_bitmap, void* cuda_stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Synthetic data generator (stands in for dbgen, scripts/genlineitem.sh)                       */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Host generator: rows [first_row, first_row+rows) of the seeded counter-based generator into
+ * reference-typed columns. Any NULL output column is skipped. */
+q1_status q1_generate_host(uint64_t seed, uint64_t first_row, uint64_t rows, q1_columns* out);
+
+/* Device generator writing compressed columns into caller-owned device buffers sized as for
+ * q1_compress_host; the pair dictionary is fixed to {AF, NF, NO, RF}. `stats` may be NULL. */
+q1_status q1_generate_compressed_device(uint64_t seed, uint64_t first_row, uint64_t rows,
+                                        q1_flag_packing packing,
+                                        const q1_compressed_host_out* dev_out,
+                                        void* cuda_stream);
+
+/* One-line description of a CUDA device (name, compute capability, SMs, memory, L2) into buf.
+ * Replaces get_device_properties / --device (src/helper.hpp:18-48, src/main.cu:266-268). */
+q1_status q1_device_describe(int32_t device, char* buf, size_t buf_len);
+
+/* Library version string. */
+const char* q1_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* Q1_H_ */

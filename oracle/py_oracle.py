@@ -1,0 +1,189 @@
+"""ctypes access to the oracle (TEST INFRASTRUCTURE).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs import this
+module; the product never does.
+
+  liboracle.so       plain-C restatement of the reference's algorithm (oracle/q1_oracle.c)
+  _ref/libq1ref.so   the reference's own CPU kernels (KernelHyPer, KernelX100), compiled from the
+                     reference sources by oracle/Makefile
+Results are numpy arrays of shape (groups, 6) holding Python ints (exact 128-bit values), in the
+aggregate order count, sum_qty (hundredths), sum_base_price, sum_disc, sum_disc_price, sum_charge.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NG, NA = 6, 6
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle not built: {path} (run make -C oracle)")
+        _lib = ctypes.CDLL(path)
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libq1ref.so"))
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libq1ref.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference oracle not built: {path}")
+        r = ctypes.CDLL(path)
+        r.q1ref_table_new.restype = ctypes.c_void_p
+        r.q1ref_table_new.argtypes = [ctypes.c_uint64]
+        r.q1ref_table_free.argtypes = [ctypes.c_void_p]
+        r.q1ref_table_push.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 7 + [ctypes.c_uint64, ctypes.c_int32]
+        r.q1ref_table_rows.restype = ctypes.c_uint64
+        r.q1ref_table_rows.argtypes = [ctypes.c_void_p]
+        r.q1ref_hyper.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        r.q1ref_x100.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+        r.q1ref_pool_new.restype = ctypes.c_void_p
+        r.q1ref_pool_new.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        r.q1ref_pool_run.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
+        r.q1ref_pool_threads.argtypes = [ctypes.c_void_p]
+        r.q1ref_pool_free.argtypes = [ctypes.c_void_p]
+        _ref = r
+    return _ref
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def i128_to_ints(buf, groups):
+    """Decode a little-endian int128 buffer of shape (groups*6*2) uint64 into Python ints."""
+    u = buf.reshape(groups, NA, 2)
+    out = np.empty((groups, NA), dtype=object)
+    for g in range(groups):
+        for a in range(NA):
+            v = int(u[g, a, 0]) | (int(u[g, a, 1]) << 64)
+            if v >= 1 << 127:
+                v -= 1 << 128
+            out[g, a] = v
+    return out
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def q1_uncompressed(cols, cutoff_day=729999):
+    n = len(cols["shipdate"])
+    buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+    L = lib()
+    L.oracle_q1_uncompressed.argtypes = [ctypes.c_void_p] * 7 + [ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p]
+    keep = [_c(cols["shipdate"], np.int32), _c(cols["discount"], np.int64), _c(cols["extendedprice"], np.int64),
+            _c(cols["tax"], np.int64), _c(cols["quantity"], np.int64),
+            _c(cols["returnflag"].view(np.uint8), np.uint8), _c(cols["linestatus"].view(np.uint8), np.uint8)]
+    flag = L.oracle_q1_uncompressed(*[ptr(k) for k in keep], n, cutoff_day, ptr(buf))
+    return i128_to_ints(buf, NG), flag
+
+
+def q1_compressed(c, cutoff_day=729999, use_filter=False):
+    n = len(c["shipdate"])
+    buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+    L = lib()
+    L.oracle_q1_compressed.argtypes = ([ctypes.c_void_p] * 5 + [ctypes.c_int] + [ctypes.c_void_p] * 5 +
+                                       [ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p])
+    pair = "flags" in c
+    filt = c.get("filter") if use_filter else None
+    keep = [_c(c["shipdate"], np.uint16), _c(c["discount"], np.uint8), _c(c["extendedprice"], np.uint32),
+            _c(c["tax"], np.uint8), _c(c["quantity"], np.uint8)]
+    flags = _c(c["flags"], np.uint32) if pair else None
+    pg = _c(c["pair_group"], np.uint8) if pair else None
+    rf = None if pair else _c(c["returnflag"], np.uint32)
+    ls = None if pair else _c(c["linestatus"], np.uint32)
+    fl = None if filt is None else _c(filt, np.uint32)
+    flag = L.oracle_q1_compressed(*[ptr(k) for k in keep], 0 if pair else 1, ptr(flags), ptr(pg), ptr(rf), ptr(ls),
+                                  ptr(fl), n, cutoff_day, ptr(buf))
+    return i128_to_ints(buf, NG), flag
+
+
+def q1_groupkey(c, keys, num_groups, cutoff_day=729999):
+    n = len(c["shipdate"])
+    buf = np.zeros(num_groups * NA * 2, dtype=np.uint64)
+    L = lib()
+    L.oracle_q1_groupkey.argtypes = ([ctypes.c_void_p] * 6 + [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32,
+                                                              ctypes.c_void_p])
+    keep = [_c(c["shipdate"], np.uint16), _c(c["discount"], np.uint8), _c(c["extendedprice"], np.uint32),
+            _c(c["tax"], np.uint8), _c(c["quantity"], np.uint8), _c(keys, np.uint32)]
+    flag = L.oracle_q1_groupkey(*[ptr(k) for k in keep], num_groups, n, cutoff_day, ptr(buf))
+    return buf.view(np.uint64), flag
+
+
+def groupkey_ints(buf, num_groups):
+    return i128_to_ints(buf, num_groups)
+
+
+def precompute_filter(c_shipdate, cutoff_day):
+    n = len(c_shipdate)
+    out = np.zeros((n + 31) // 32, dtype=np.uint32)
+    L = lib()
+    L.oracle_precompute_filter.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p]
+    s = _c(c_shipdate, np.uint16)
+    L.oracle_precompute_filter(ptr(s), n, cutoff_day, ptr(out))
+    return out
+
+
+class RefTable:
+    """The reference's lineitem (cpu/tpch_kit.hpp:135-149) filled through Column::Push."""
+
+    def __init__(self, cols, cutoff_day=729999):
+        r = ref()
+        n = len(cols["shipdate"])
+        self.n = n
+        self.h = r.q1ref_table_new(max(n, 1))
+        keep = [_c(cols["shipdate"], np.int32), _c(cols["discount"], np.int64), _c(cols["extendedprice"], np.int64),
+                _c(cols["tax"], np.int64), _c(cols["quantity"], np.int64),
+                _c(cols["returnflag"].view(np.uint8), np.uint8), _c(cols["linestatus"].view(np.uint8), np.uint8)]
+        r.q1ref_table_push(self.h, *[ptr(k) for k in keep], n, cutoff_day)
+        self.pool = None
+
+    def hyper(self):
+        buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+        flag = ref().q1ref_hyper(self.h, ptr(buf))
+        return i128_to_ints(buf, NG), flag
+
+    def x100(self, offset=0, num=None):
+        num = self.n - offset if num is None else num
+        buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+        rc = ref().q1ref_x100(self.h, offset, num, ptr(buf))
+        return i128_to_ints(buf, NG), rc
+
+    def x100_parallel(self, threads, offset=0, num=None, morsel=1 << 16):
+        num = self.n - offset if num is None else num
+        if self.pool is None:
+            self.pool = ref().q1ref_pool_new(self.h, threads)
+        buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+        rc = ref().q1ref_pool_run(self.pool, offset, num, morsel, ptr(buf))
+        return i128_to_ints(buf, NG), rc
+
+    def threads(self):
+        return ref().q1ref_pool_threads(self.pool) if self.pool else 0
+
+    def close(self):
+        if self.pool is not None:
+            ref().q1ref_pool_free(self.pool)
+            self.pool = None
+        if self.h:
+            ref().q1ref_table_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,135 @@
+"""Host logic of the product (no GPU compute): generator, compressor, filter bitmap, placement
+names, parameter validation, result finalisation. Every check is against an independent
+restatement (tests/gen_np.py) or the oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import gen_np
+import tpchq01_gpu_b200 as q
+from oracle import py_oracle as O
+from tpchq01_gpu_b200 import _lib
+
+
+@pytest.mark.parametrize("seed,first,rows", [(1, 0, 1), (7, 100, 100_000), (20260101, 5_000_000, 33_333)])
+def test_host_generator_equals_numpy_restatement(seed, first, rows):
+    a = q.generate_host(seed, first, rows)
+    b = gen_np.generate(seed, first, rows)
+    for k in b:
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+
+
+def test_generator_distribution_matches_spec():
+    c = gen_np.generate(99, 0, 200_000)
+    ship = c["shipdate"]
+    assert ship.min() >= 727563 + 1 and ship.max() <= 729968 + 121
+    assert set(np.unique(c["discount"])) <= set(range(11))
+    assert set(np.unique(c["tax"])) <= set(range(9))
+    assert set(np.unique(c["quantity"] // 100)) == set(range(1, 51))
+    pairs = set(zip(c["returnflag"].tolist(), c["linestatus"].tolist()))
+    assert pairs == {(b"A", b"F"), (b"N", b"F"), (b"N", b"O"), (b"R", b"F")}
+
+
+@pytest.mark.parametrize("packing", ["pair", "separate"])
+def test_compressor_equals_restatement(packing):
+    cols = gen_np.generate(5, 0, 50_001)
+    got, st = q.compress_host(cols, packing)
+    ref = gen_np.compress(cols, "pair" if packing == "pair" else "sep")
+    for k, v in ref.items():
+        if k == "num_pair_codes":
+            assert got[k] == v
+        else:
+            assert np.array_equal(np.asarray(got[k]), np.asarray(v)), k
+    assert st.rows == 50_001 and st.max_discount <= 10 and st.max_quantity <= 50
+    if packing == "separate":
+        # also equal to the oracle's restatement of src/main.cu:773-803
+        n = 50_001
+        bufs = dict(s=np.zeros(n, np.uint16), d=np.zeros(n, np.uint8), p=np.zeros(n, np.uint32),
+                    t=np.zeros(n, np.uint8), q=np.zeros(n, np.uint8), rf=np.zeros((n + 15) // 16, np.uint32),
+                    ls=np.zeros((n + 31) // 32, np.uint32))
+        L = O.lib()
+        L.oracle_compress_separate.argtypes = [ctypes.c_void_p] * 7 + [ctypes.c_uint64] + [ctypes.c_void_p] * 7
+        keep = [cols["shipdate"], cols["discount"], cols["extendedprice"], cols["tax"], cols["quantity"],
+                cols["returnflag"].view(np.uint8), cols["linestatus"].view(np.uint8)]
+        bad = L.oracle_compress_separate(*[O.ptr(k) for k in keep], n, *[O.ptr(bufs[k]) for k in
+                                                                          ["s", "d", "p", "t", "q", "rf", "ls"]])
+        assert bad == 0
+        assert np.array_equal(bufs["rf"], got["returnflag"]) and np.array_equal(bufs["ls"], got["linestatus"])
+
+
+@pytest.mark.parametrize("field,value,msg", [
+    ("discount", 101, "discount"), ("tax", 300, "tax"), ("quantity", 150, "quantity"),
+    ("shipdate", 727000, "shipdate"), ("extendedprice", 1 << 33, "extendedprice"), ("returnflag", b"X", "returnflag")])
+def test_compressor_rejects_out_of_domain(field, value, msg):
+    cols = gen_np.generate(6, 0, 100)
+    cols[field][42] = value
+    with pytest.raises(q.Q1Error) as e:
+        q.compress_host(cols, "pair")
+    assert e.value.status == 6 and msg in e.value.message and "row 42" in e.value.message
+
+
+def test_pair_packing_rejects_more_than_four_combinations():
+    cols = gen_np.generate(6, 0, 100)
+    cols["returnflag"][0], cols["linestatus"][0] = b"A", b"O"
+    cols["returnflag"][1], cols["linestatus"][1] = b"R", b"O"
+    with pytest.raises(q.Q1Error):
+        q.compress_host(cols, "pair")
+    q.compress_host(cols, "separate")
+
+
+def test_filter_bitmap_host():
+    cols = gen_np.generate(8, 0, 10_007)
+    c = gen_np.compress(cols)
+    for cut in [727000, 728826, 729999, 731000]:
+        assert np.array_equal(q.precompute_filter_host(c["shipdate"], cut), gen_np.filter_bitmap(c["shipdate"], cut))
+
+
+@pytest.mark.parametrize("name,idx", [("in_registers", 0), ("in-registers", 0), ("in_registers_per_thread", 1),
+                                      ("local_mem", 2), ("local-mem", 2), ("shared_mem_per_thread", 3),
+                                      ("per-thread-shared-mem", 3), ("global", 4)])
+def test_placement_names_both_spellings(name, idx):
+    assert q.placement_id(name) == idx
+
+
+def test_unknown_placement_message():
+    with pytest.raises(q.Q1Error) as e:
+        q.placement_id("shared_mem")
+    assert 'No kernel variant named "shared_mem"' in e.value.message
+
+
+@pytest.mark.parametrize("kw,fragment", [
+    (dict(use_filter_pushdown=True), "only currently supported when compression is applied"),
+    (dict(num_threads_per_block=100), "multiples of the warp size"),
+    (dict(num_query_execution_runs=0), "Number of runs must be positive"),
+    (dict(cpu_processing_fraction=1.5), "range 0.0 - 1.0"),
+    (dict(num_tuples_per_kernel_launch=1000), "multiple of 128"),
+    (dict(num_gpu_streams=0), "streams"),
+])
+def test_params_validation_like_reference(kw, fragment):
+    with pytest.raises(q.Q1Error) as e:
+        q.Q1Params(**kw).validate()
+    assert fragment in e.value.message
+
+
+def test_params_defaults_are_reference_defaults():
+    p = _lib.Params()
+    q.lib().q1_params_default(ctypes.byref(p))
+    assert p.placement == 1 and p.streams == 4 and p.tuples_per_launch == 1 << 21 and p.runs == 5
+    assert p.cpu_fraction == 0.5 and p.cutoff_day == 729999
+    q.Q1Params(apply_compression=True, use_filter_pushdown=True).validate()
+
+
+def test_finalize_averages_truncate_toward_zero():
+    aggs = (_lib.I128 * 36)()
+    def put(g, a, v):
+        v &= (1 << 128) - 1
+        aggs[g * 6 + a].lo = v & ((1 << 64) - 1)
+        aggs[g * 6 + a].hi = v >> 64
+    put(0, 0, 3); put(0, 1, 1000); put(0, 2, -1000); put(0, 3, 7)
+    put(1, 0, 0); put(1, 1, 5)
+    out = (_lib.GroupResult * 6)()
+    _lib.check(q.lib().q1_finalize_groups(aggs, 6, out))
+    assert out[0].avg_qty_e4 == 33333 and out[0].avg_price_e4 == -33333 and out[0].avg_disc_e4 == 233
+    assert out[1].avg_qty_e4 == 0 and out[0].returnflag == b"A" and out[3].linestatus == b"O"
+    assert out[0].sum_base_price.value() == -1000

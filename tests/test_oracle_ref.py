@@ -1,0 +1,35 @@
+"""The oracle against the reference's own CPU kernels run live (oracle/_ref/libq1ref.so) on
+fresh seeded inputs: KernelHyPer<true>, KernelX100 single-threaded and on a thread pool."""
+import numpy as np
+import pytest
+
+import gen_np
+from oracle import py_oracle as O
+
+pytestmark = pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+
+
+@pytest.mark.parametrize("seed,rows,cutoff", [(101, 200_000, 729999), (102, 77_777, 729906),
+                                              (103, 50_000, 730089), (104, 65_536, 728500)])
+def test_restatement_equals_reference_kernels(seed, rows, cutoff):
+    cols = gen_np.generate(seed, 0, rows)
+    mine, f1 = O.q1_uncompressed(cols, cutoff)
+    t = O.RefTable(cols, cutoff)
+    hyper, f2 = t.hyper()
+    x100, rc = t.x100()
+    par, rc2 = t.x100_parallel(3, morsel=4096)
+    t.close()
+    assert f1 == 0 and f2 == 0 and rc == 0 and rc2 == 0
+    assert np.array_equal(mine, hyper)
+    assert np.array_equal(mine, x100)
+    assert np.array_equal(mine, par)
+
+
+def test_x100_partial_ranges_add_up():
+    cols = gen_np.generate(105, 0, 30_000)
+    t = O.RefTable(cols)
+    a, _ = t.x100(0, 10_000)
+    b, _ = t.x100(10_000, 20_000)
+    whole, _ = t.x100()
+    t.close()
+    assert np.array_equal(a + b, whole)

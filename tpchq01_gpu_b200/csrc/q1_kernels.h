@@ -1,0 +1,69 @@
+// Internal interface between the host runtime (C++) and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace q1 {
+
+// Input layouts the scan kernel understands (column order inside a tile in brackets).
+enum ScanLayout : int {
+    kLayPair = 0,        // [ship u16, qty u8, disc u8, tax u8, price u32, pair code 2b]
+    kLayPairFilter = 1,  // [filter 1b, qty, disc, tax, price, pair code 2b]
+    kLaySep = 2,         // [ship u16, qty, disc, tax, price, rf 2b, ls 1b]
+    kLaySepFilter = 3,   // [filter 1b, qty, disc, tax, price, rf 2b, ls 1b]
+    kLayUncomp = 4,      // [ship i32, qty i64, disc i64, tax i64, price i64, rf char, ls char]
+    kNumScanLayouts = 5
+};
+
+// Table placements (same numbering as q1_placement in include/q1.h).
+enum ScanPlacement : int {
+    kPlaceInRegisters = 0,
+    kPlaceInRegistersPerThread = 1,
+    kPlaceLocalMem = 2,
+    kPlaceSharedMemPerThread = 3,
+    kPlaceGlobal = 4,
+};
+
+// Rows per tile (one bulk copy per column per tile); a multiple of 128 so that every column
+// slice of every tile starts on a 16-byte boundary, down to 1-bit columns.
+template <int L>
+inline constexpr uint32_t kTileRows = (L == kLayUncomp) ? 1024u : 4096u;
+// Shared-memory ring depth.
+template <int L, int P>
+inline constexpr uint32_t kStages = (P == kPlaceSharedMemPerThread) ? 3u : 4u;
+// Consumer warps per CTA (plus one producer warp).
+inline constexpr uint32_t kConsumerWarps = 8;
+
+struct ScanParams {
+    const uint8_t* col[7];      // column base pointers in tile order; 16-byte aligned
+    uint64_t rows;              // rows to aggregate (<= 2^31 per launch)
+    int32_t cutoff;             // compressed: cutoff_day - 727563; uncompressed: cutoff_day
+    uint32_t qty_scale;         // 100 when quantity is stored in whole units, else 1
+    uint8_t pair_group[4];      // pair layouts: code -> group
+    unsigned long long* out;    // [6 groups][6 aggregates][lo, hi]
+    uint32_t* status;           // device status word (kStatus* bits); may be null
+};
+
+// Launch the scan kernel for one layout x placement. max_blocks <= 0: one CTA per SM.
+cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm_count, int max_blocks,
+                        cudaStream_t stream);
+uint32_t scan_tile_rows(int layout);
+
+// Utility kernels (util_kernels.cu).
+struct GenCompressedOut {
+    uint16_t* shipdate;
+    uint8_t* discount;
+    uint32_t* extendedprice;
+    uint8_t* tax;
+    uint8_t* quantity;
+    uint32_t* flags;        // pair codes (may be null)
+    uint32_t* returnflag;   // separate containers (may be null)
+    uint32_t* linestatus;
+};
+cudaError_t launch_generate_compressed(uint64_t seed, uint64_t first_row, uint64_t rows, const GenCompressedOut& out,
+                                       cudaStream_t stream);
+cudaError_t launch_precompute_filter(const uint16_t* shipdate, uint64_t rows, int32_t cutoff_rel, uint32_t* bitmap,
+                                     cudaStream_t stream);
+
+}  // namespace q1

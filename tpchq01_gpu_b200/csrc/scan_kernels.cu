@@ -1,0 +1,659 @@
+// Q1 scan kernels for sm_100a: date predicate + (returnflag, linestatus) group-by with exact
+// fixed-point sums, over HBM-resident columns.
+//
+// Replaces the 15 __global__ kernels of the reference (src/kernels/*: 5 table placements x
+// {uncompressed, compressed, filter-pushdown compressed}); the per-row arithmetic is that of
+// every reference kernel (e.g. src/kernels/ht_in_registers_per_thread.cuh:38-60):
+//   disc_1 = 100 - disc, disc_price = disc_1 * price, charge = disc_price * (100 + tax),
+//   group = (rf << 1) + ls; sums of quantity, price, disc_price, charge, disc and a count.
+//
+// Structure (one design for every layout and placement):
+//   * persistent grid, one CTA per SM, each CTA = 1 producer warp + W consumer warps;
+//   * the producer streams tiles of R rows, every column of the tile with one
+//     cp.async.bulk (TMA bulk copy, evict-first L2 policy) into an S-stage shared-memory ring,
+//     completion tracked on mbarriers; consumers release a stage with one arrive per warp;
+//   * consumers decode the rows from shared memory in registers (predicate, group code,
+//     quantity/discount/tax bytes, price) and accumulate according to the placement;
+//   * one 128-bit atomic per CTA per (group, aggregate) into the caller's buffer.
+// Every wait is bounded (q1_ptx.cuh, kWaitLimitNs); on expiry the kernel records
+// kStatusWaitTimeout in the status word, drains its own copies and returns.
+//
+// Domain: discount <= 100 (so 100 - d >= 0), tax <= 255, extendedprice and quantity < 2^32.
+// Then every per-row product fits 64 bits unsigned (charge < 2^47.2) and per-thread 64-bit
+// partials cannot wrap for launches of up to 2^31 rows (the host splits longer launches).
+// A row outside the domain sets kStatusDomain (the host reports Q1_ERR_DOMAIN).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "q1_common.cuh"
+#include "q1_kernels.h"
+#include "q1_ptx.cuh"
+
+namespace q1 {
+
+using namespace ptx;
+
+// ---------------------------------------------------------------------------------------------
+// Layouts
+// ---------------------------------------------------------------------------------------------
+
+// Column order inside a tile: ship (or filter), qty, disc, tax, price, flags... (see q1_kernels.h)
+template <int L>
+struct LayoutTraits;
+
+template <>
+struct LayoutTraits<kLayPair> {
+    static constexpr int kCols = 6;
+    static constexpr uint64_t kBitsWord = 0x0000022008080810ull;  // bits per column, one byte each: {16, 8, 8, 8, 32, 2, 0}
+    static constexpr int kRowsPerStep = 4;
+    static constexpr int kCodes = 4;   // 2-bit pair dictionary
+    static constexpr bool kFilter = false;
+    static constexpr bool kWideQty = false;
+};
+template <>
+struct LayoutTraits<kLayPairFilter> {
+    static constexpr int kCols = 6;
+    static constexpr uint64_t kBitsWord = 0x0000022008080801ull;  // bits per column, one byte each: {1, 8, 8, 8, 32, 2, 0}
+    static constexpr int kRowsPerStep = 4;
+    static constexpr int kCodes = 4;
+    static constexpr bool kFilter = true;
+    static constexpr bool kWideQty = false;
+};
+template <>
+struct LayoutTraits<kLaySep> {
+    static constexpr int kCols = 7;
+    static constexpr uint64_t kBitsWord = 0x0001022008080810ull;  // bits per column, one byte each: {16, 8, 8, 8, 32, 2, 1}
+    static constexpr int kRowsPerStep = 4;
+    static constexpr int kCodes = 6;   // (rf << 1) + ls
+    static constexpr bool kFilter = false;
+    static constexpr bool kWideQty = false;
+};
+template <>
+struct LayoutTraits<kLaySepFilter> {
+    static constexpr int kCols = 7;
+    static constexpr uint64_t kBitsWord = 0x0001022008080801ull;  // bits per column, one byte each: {1, 8, 8, 8, 32, 2, 1}
+    static constexpr int kRowsPerStep = 4;
+    static constexpr int kCodes = 6;
+    static constexpr bool kFilter = true;
+    static constexpr bool kWideQty = false;
+};
+template <>
+struct LayoutTraits<kLayUncomp> {
+    static constexpr int kCols = 7;
+    static constexpr uint64_t kBitsWord = 0x0008084040404020ull;  // bits per column, one byte each: {32, 64, 64, 64, 64, 8, 8}
+    static constexpr int kRowsPerStep = 2;
+    static constexpr int kCodes = 6;
+    static constexpr bool kFilter = false;
+    static constexpr bool kWideQty = true;
+};
+
+template <int L>
+__host__ __device__ constexpr uint32_t col_bits(int c) {
+    return (uint32_t)((LayoutTraits<L>::kBitsWord >> (8 * c)) & 0xFFu);
+}
+template <int L>
+__host__ __device__ constexpr uint32_t col_offset(int c, uint32_t R) {
+    uint32_t off = 0;
+    for (int i = 0; i < c; ++i) off += R * col_bits<L>(i) / 8u;
+    return off;
+}
+template <int L>
+__host__ __device__ constexpr uint32_t stage_bytes(uint32_t R) {
+    return col_offset<L>(LayoutTraits<L>::kCols, R);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Accumulators (table placements)
+// ---------------------------------------------------------------------------------------------
+
+// Per-row decoded values handed to a placement:
+//   c  group code (0..kCodes-1) of a passing row, or a value >= kCodes for a filtered row
+//   q  quantity (whole units for compressed, hundredths for uncompressed)
+//   d  discount, a = 100 - d, ab = a * (100 + tax), p = extendedprice
+
+// Aggregates of one group, per thread, in registers.
+template <bool kWideQty>
+struct GroupRegs {
+    uint64_t p, dp, ch;
+    uint64_t qd64;      // packed: sum q (low 32) | sum d (high 32)   [!kWideQty]
+    uint64_t q64;       // sum q                                      [kWideQty]
+    uint32_t qd, d32, cnt;
+
+    __device__ __forceinline__ void zero() {
+        p = dp = ch = qd64 = q64 = 0;
+        qd = d32 = cnt = 0;
+    }
+    __device__ __forceinline__ void add(bool hit, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t pr) {
+        const uint32_t pg = hit ? pr : 0u;
+        if (kWideQty) {
+            q64 = mad_wide(hit ? q : 0u, 1u, q64);
+            d32 += hit ? d : 0u;
+        } else {
+            qd += hit ? (q | (d << 16)) : 0u;
+        }
+        cnt += hit ? 1u : 0u;
+        p += pg;
+        dp = mad_wide(a, pg, dp);
+        ch = mad_wide(ab, pg, ch);
+    }
+    // Move the 16-bit packed partials into 64 bits; needed at least every 256 rows.
+    __device__ __forceinline__ void fold() {
+        if (!kWideQty) {
+            qd64 += (uint64_t)(qd & 0xFFFFu) | ((uint64_t)(qd >> 16) << 32);
+            qd = 0;
+        }
+    }
+    // Aggregate values in q1 order (count, qty, price, disc, disc_price, charge); after fold().
+    __device__ __forceinline__ uint64_t value(int agg) const {
+        switch (agg) {
+            case kAggCount: return cnt;
+            case kAggQty: return kWideQty ? q64 : (qd64 & 0xFFFFFFFFull);
+            case kAggBasePrice: return p;
+            case kAggDisc: return kWideQty ? (uint64_t)d32 : (qd64 >> 32);
+            case kAggDiscPrice: return dp;
+            default: return ch;
+        }
+    }
+};
+
+// Shared-memory reduction target of a CTA: [codes][6] x (lo, hi).
+struct CtaRed {
+    unsigned long long* v;
+    __device__ __forceinline__ void add(int code, int agg, uint64_t lo, uint64_t hi) {
+        atomic_add_u128_shared(v + 2 * (code * kNumAggs + agg), lo, hi);
+    }
+};
+
+// --- in_registers_per_thread: every thread owns all groups in registers; a row updates the
+// matching group through predicated (select) arithmetic over all groups
+// (src/kernels/ht_in_registers_per_thread.cuh:11-79).
+template <int G, bool kWideQty>
+struct AccPerThread {
+    GroupRegs<kWideQty> g[G];
+    __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
+#pragma unroll
+        for (int i = 0; i < G; ++i) g[i].zero();
+    }
+    __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
+#pragma unroll
+        for (int i = 0; i < G; ++i) g[i].add(c == (uint32_t)i, q, d, a, ab, p);
+    }
+    __device__ __forceinline__ void fold() {
+#pragma unroll
+        for (int i = 0; i < G; ++i) g[i].fold();
+    }
+    template <class P>
+    __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
+        fold();
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+#pragma unroll
+            for (int a = 0; a < kNumAggs; ++a) {
+                uint64_t lo = g[i].value(a), hi = 0;
+                warp_sum_u128(lo, hi);
+                if (lane == 0) red.add(i, a, lo, hi);
+            }
+        }
+    }
+};
+
+// --- in_registers ("warp-lane tables", src/kernels/ht_in_registers.cuh:30-121): the lanes of a
+// warp form floor(32/G) tables of G lanes; lane (table, g) keeps only group g in registers; all
+// G lanes of a table read the same rows (a shared-memory broadcast, so unlike the reference no
+// row is fetched from DRAM more than once) and each adds the rows of its own group.
+template <int G, bool kWideQty>
+struct AccWarpLane {
+    GroupRegs<kWideQty> r;
+    uint32_t my;
+    __device__ __forceinline__ void init(uint32_t lane, uint32_t, uint8_t*) {
+        r.zero();
+        my = lane % G;
+    }
+    __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
+        r.add(c == my, q, d, a, ab, p);
+    }
+    __device__ __forceinline__ void fold() { r.fold(); }
+    template <class P>
+    __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
+        fold();
+        if (lane < (32u / G) * G) {
+#pragma unroll
+            for (int a = 0; a < kNumAggs; ++a) red.add((int)my, a, r.value(a), 0);
+        }
+    }
+};
+
+// --- local_mem (src/kernels/ht_in_local_mem.cuh:11-74): per-thread tables indexed by the row's
+// group, which places them in (L1-cached) local memory.
+template <int G, bool kWideQty>
+struct AccLocal {
+    uint64_t t[G][5];   // p, dp, ch, q, d
+    uint32_t cnt[G];
+    __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
+        for (int i = 0; i < G; ++i) {
+            for (int j = 0; j < 5; ++j) t[i][j] = 0;
+            cnt[i] = 0;
+        }
+    }
+    __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
+        if (c < (uint32_t)G) {
+            t[c][0] += p;
+            t[c][1] = mad_wide(a, p, t[c][1]);
+            t[c][2] = mad_wide(ab, p, t[c][2]);
+            t[c][3] += q;
+            t[c][4] += d;
+            cnt[c] += 1;
+        }
+    }
+    __device__ __forceinline__ void fold() {}
+    template <class P>
+    __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            const uint64_t vals[kNumAggs] = {cnt[i], t[i][3], t[i][0], t[i][4], t[i][1], t[i][2]};
+#pragma unroll
+            for (int a = 0; a < kNumAggs; ++a) {
+                uint64_t lo = vals[a], hi = 0;
+                warp_sum_u128(lo, hi);
+                if (lane == 0) red.add(i, a, lo, hi);
+            }
+        }
+    }
+};
+
+// --- shared_mem_per_thread (src/kernels/ht_in_shared_mem_per_thread.cuh:23-118): per-thread
+// tables in shared memory, laid out [field][group][thread] so a warp's accesses are
+// bank-conflict free.
+template <int G, bool kWideQty>
+struct AccSharedPerThread {
+    uint64_t* tab;       // 5 * G * T entries
+    uint32_t* cnt;       // G * T entries
+    uint32_t tid, nthreads;
+    __device__ __forceinline__ void init(uint32_t, uint32_t consumer_tid, uint8_t* scratch) {
+        tid = consumer_tid;
+        nthreads = blockDim.x - 32;
+        tab = reinterpret_cast<uint64_t*>(scratch);
+        cnt = reinterpret_cast<uint32_t*>(tab + 5 * G * nthreads);
+        for (int i = 0; i < 5 * G; ++i) tab[i * nthreads + tid] = 0;
+        for (int i = 0; i < G; ++i) cnt[i * nthreads + tid] = 0;
+    }
+    __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
+        if (c < (uint32_t)G) {
+            const uint32_t base = c * nthreads + tid;
+            const uint32_t stride = G * nthreads;
+            tab[base] += p;
+            tab[base + stride] = mad_wide(a, p, tab[base + stride]);
+            tab[base + 2 * stride] = mad_wide(ab, p, tab[base + 2 * stride]);
+            tab[base + 3 * stride] += q;
+            tab[base + 4 * stride] += d;
+            cnt[base] += 1;
+        }
+    }
+    __device__ __forceinline__ void fold() {}
+    template <class P>
+    __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
+        const uint32_t stride = G * nthreads;
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            const uint32_t base = i * nthreads + tid;
+            const uint64_t vals[kNumAggs] = {cnt[base], tab[base + 3 * stride], tab[base], tab[base + 4 * stride],
+                                             tab[base + stride], tab[base + 2 * stride]};
+#pragma unroll
+            for (int a = 0; a < kNumAggs; ++a) {
+                uint64_t lo = vals[a], hi = 0;
+                warp_sum_u128(lo, hi);
+                if (lane == 0) red.add(i, a, lo, hi);
+            }
+        }
+    }
+};
+
+// --- global (src/kernels/ht_in_global_mem.hpp:11-52): no thread- or block-private table; the
+// aggregates live only in the global output. The reference issues 6 atomics per row; here each
+// warp first combines its rows of one tile (a register buffer emptied after every tile) and then
+// issues one 64-bit atomic per (group, aggregate) straight into the global table.
+template <int G, bool kWideQty>
+struct AccGlobal {
+    AccPerThread<G, kWideQty> buf;
+    __device__ __forceinline__ void init(uint32_t a, uint32_t b, uint8_t* s) { buf.init(a, b, s); }
+    __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
+        buf.add(c, q, d, a, ab, p);
+    }
+    __device__ __forceinline__ void fold() { buf.fold(); }
+    template <class P>
+    __device__ __forceinline__ void tile_done(const P& prm, uint32_t lane) {
+        buf.fold();
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+            const int grp = G == 4 ? prm.pair_group[i] : i;
+#pragma unroll
+            for (int a = 0; a < kNumAggs; ++a) {
+                uint64_t v = warp_sum_u64(buf.g[i].value(a));
+                if (a == kAggQty) v *= prm.qty_scale;
+                if (lane == (uint32_t)((i * kNumAggs + a) & 31)) atomic_add_u128(prm.out + 2 * (grp * kNumAggs + a), v, 0);
+            }
+            buf.g[i].zero();
+        }
+    }
+    __device__ __forceinline__ void flush(CtaRed, uint32_t) {}
+};
+
+template <int P, int G, bool W>
+struct AccSel;
+template <int G, bool W> struct AccSel<kPlaceInRegisters, G, W> { using T = AccWarpLane<G, W>; };
+template <int G, bool W> struct AccSel<kPlaceInRegistersPerThread, G, W> { using T = AccPerThread<G, W>; };
+template <int G, bool W> struct AccSel<kPlaceLocalMem, G, W> { using T = AccLocal<G, W>; };
+template <int G, bool W> struct AccSel<kPlaceSharedMemPerThread, G, W> { using T = AccSharedPerThread<G, W>; };
+template <int G, bool W> struct AccSel<kPlaceGlobal, G, W> { using T = AccGlobal<G, W>; };
+
+// ---------------------------------------------------------------------------------------------
+// Row decoding
+// ---------------------------------------------------------------------------------------------
+
+// Any byte of a discount word above 100 (top bit of (b & 0x7F) + 27, or b >= 128).
+__device__ __forceinline__ uint32_t disc_out_of_domain4(uint32_t D) {
+    return (((D & 0x7F7F7F7Fu) + 0x1B1B1B1Bu) | D) & 0x80808080u;
+}
+
+__device__ __forceinline__ uint32_t code_of_chars(uint32_t rf, uint32_t ls) {
+    const uint32_t r = (rf == 'R' ? 2u : 0u) + (rf == 'N' ? 1u : 0u);
+    return (r << 1) + (ls == 'F' ? 0u : 1u);
+}
+
+// One step of rows [kRowsPerStep * j, +kRowsPerStep) of the tile held at shared address `base`.
+template <int L, class Acc>
+__device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t cut, Acc& acc, uint32_t& bad) {
+    using T = LayoutTraits<L>;
+    constexpr uint32_t R = kTileRows<L>;
+    if constexpr (L == kLayUncomp) {
+        const uint2 sd = lds_v2(base + col_offset<L>(0, R) + 8 * j);
+        const uint4 Q = lds_v4(base + col_offset<L>(1, R) + 16 * j);
+        const uint4 D = lds_v4(base + col_offset<L>(2, R) + 16 * j);
+        const uint4 X = lds_v4(base + col_offset<L>(3, R) + 16 * j);
+        const uint4 P = lds_v4(base + col_offset<L>(4, R) + 16 * j);
+        const uint32_t RF = lds_u16(base + col_offset<L>(5, R) + 2 * j);
+        const uint32_t LS = lds_u16(base + col_offset<L>(6, R) + 2 * j);
+        bad |= Q.y | Q.w | D.y | D.w | X.y | X.w | P.y | P.w;
+        bad |= (D.x > 100u) | (D.z > 100u) | (X.x > 255u) | (X.z > 255u);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int32_t ship = (int32_t)(r ? sd.y : sd.x);
+            const uint32_t code = code_of_chars((RF >> (8 * r)) & 0xFFu, (LS >> (8 * r)) & 0xFFu);
+            const uint32_t c = ship <= cut ? code : 7u;
+            const uint32_t q = r ? Q.z : Q.x;
+            const uint32_t d = r ? D.z : D.x;
+            const uint32_t t = r ? X.z : X.x;
+            const uint32_t p = r ? P.z : P.x;
+            const uint32_t a = 100u - d;
+            acc.add(c, q, d, a, a * (100u + t), p);
+        }
+    } else {
+        constexpr bool kSep = (L == kLaySep || L == kLaySepFilter);
+        uint32_t passbits;
+        if constexpr (T::kFilter) {
+            passbits = lds_u8(base + col_offset<L>(0, R) + (j >> 1)) >> ((j & 1u) * 4u);
+        } else {
+            const uint2 sd = lds_v2(base + col_offset<L>(0, R) + 8 * j);
+            passbits = ((int32_t)(sd.x & 0xFFFFu) <= cut ? 1u : 0u) | ((int32_t)(sd.x >> 16) <= cut ? 2u : 0u) |
+                       ((int32_t)(sd.y & 0xFFFFu) <= cut ? 4u : 0u) | ((int32_t)(sd.y >> 16) <= cut ? 8u : 0u);
+        }
+        const uint32_t Q = lds_u32(base + col_offset<L>(1, R) + 4 * j);
+        const uint32_t D = lds_u32(base + col_offset<L>(2, R) + 4 * j);
+        const uint32_t X = lds_u32(base + col_offset<L>(3, R) + 4 * j);
+        const uint4 P = lds_v4(base + col_offset<L>(4, R) + 16 * j);
+        uint32_t F, LS = 0;
+        F = lds_u8(base + col_offset<L>(5, R) + j);
+        if constexpr (kSep) LS = lds_u8(base + col_offset<L>(6, R) + (j >> 1)) >> ((j & 1u) * 4u);
+        bad |= disc_out_of_domain4(D);
+        const uint32_t A = 0x64646464u - D;   // 100 - d per byte (no borrow inside the domain)
+        const uint32_t pv[4] = {P.x, P.y, P.z, P.w};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            uint32_t code;
+            if constexpr (kSep) code = (((F >> (2 * r)) & 3u) << 1) | ((LS >> r) & 1u);
+            else code = (F >> (2 * r)) & 3u;
+            const uint32_t c = ((passbits >> r) & 1u) ? code : 7u;
+            const uint32_t q = (Q >> (8 * r)) & 0xFFu;
+            const uint32_t d = (D >> (8 * r)) & 0xFFu;
+            const uint32_t a = (A >> (8 * r)) & 0xFFu;
+            const uint32_t t = (X >> (8 * r)) & 0xFFu;
+            acc.add(c, q, d, a, a * (100u + t), pv[r]);
+        }
+    }
+}
+
+// One row straight from global memory (tail rows that do not fill a tile).
+template <int L, class Acc>
+__device__ __forceinline__ void process_row_global(const ScanParams& prm, uint64_t i, Acc& acc, uint32_t& bad) {
+    if constexpr (L == kLayUncomp) {
+        const int32_t ship = __ldg(reinterpret_cast<const int32_t*>(prm.col[0]) + i);
+        const uint64_t q = __ldg(reinterpret_cast<const unsigned long long*>(prm.col[1]) + i);
+        const uint64_t d = __ldg(reinterpret_cast<const unsigned long long*>(prm.col[2]) + i);
+        const uint64_t t = __ldg(reinterpret_cast<const unsigned long long*>(prm.col[3]) + i);
+        const uint64_t p = __ldg(reinterpret_cast<const unsigned long long*>(prm.col[4]) + i);
+        const uint32_t rf = (uint8_t)__ldg(reinterpret_cast<const char*>(prm.col[5]) + i);
+        const uint32_t ls = (uint8_t)__ldg(reinterpret_cast<const char*>(prm.col[6]) + i);
+        bad |= (uint32_t)((q | p) >> 32) | (d > 100u) | (t > 255u);
+        const uint32_t c = ship <= prm.cutoff ? code_of_chars(rf, ls) : 7u;
+        const uint32_t a = 100u - (uint32_t)d;
+        acc.add(c, (uint32_t)q, (uint32_t)d, a, a * (100u + (uint32_t)t), (uint32_t)p);
+    } else {
+        using T = LayoutTraits<L>;
+        constexpr bool kSep = (L == kLaySep || L == kLaySepFilter);
+        bool pass;
+        if constexpr (T::kFilter) {
+            pass = (__ldg(reinterpret_cast<const uint32_t*>(prm.col[0]) + (i >> 5)) >> (i & 31)) & 1u;
+        } else {
+            pass = (int32_t)__ldg(reinterpret_cast<const uint16_t*>(prm.col[0]) + i) <= prm.cutoff;
+        }
+        const uint32_t q = __ldg(prm.col[1] + i);
+        const uint32_t d = __ldg(prm.col[2] + i);
+        const uint32_t t = __ldg(prm.col[3] + i);
+        const uint32_t p = __ldg(reinterpret_cast<const uint32_t*>(prm.col[4]) + i);
+        uint32_t code;
+        const uint32_t rfw = __ldg(reinterpret_cast<const uint32_t*>(prm.col[5]) + (i >> 4));
+        code = (rfw >> (2 * (i & 15))) & 3u;
+        if constexpr (kSep) {
+            const uint32_t lsw = __ldg(reinterpret_cast<const uint32_t*>(prm.col[6]) + (i >> 5));
+            code = (code << 1) | ((lsw >> (i & 31)) & 1u);
+        }
+        bad |= d > 100u;
+        const uint32_t c = pass ? code : 7u;
+        const uint32_t a = 100u - d;
+        acc.add(c, q, d, a, a * (100u + t), p);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The kernel
+// ---------------------------------------------------------------------------------------------
+
+template <int L, int P>
+__global__ void __launch_bounds__((kConsumerWarps + 1) * 32, 1)
+q1_scan_kernel(const __grid_constant__ ScanParams prm) {
+    using T = LayoutTraits<L>;
+    constexpr uint32_t R = kTileRows<L>;
+    constexpr uint32_t S = kStages<L, P>;
+    constexpr uint32_t W = kConsumerWarps;
+    constexpr uint32_t kStage = stage_bytes<L>(R);
+    constexpr int G = T::kCodes;
+    static_assert(kStage % 16 == 0, "stage must keep 16-byte alignment");
+
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full_bar[S];
+    __shared__ __align__(8) uint64_t empty_bar[S];
+    __shared__ __align__(16) unsigned long long red[G * kNumAggs * 2];
+
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t num_tiles = prm.rows / R;
+    const uint32_t ring = ptx::smem_addr(smem);
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < S; ++s) {
+            mbar_init(smem_addr(&full_bar[s]), 1);
+            mbar_init(smem_addr(&empty_bar[s]), W);
+        }
+        fence_mbar_init();
+    }
+    for (uint32_t i = threadIdx.x; i < (uint32_t)(G * kNumAggs * 2); i += blockDim.x) red[i] = 0;
+    __syncthreads();
+
+    if (warp == W) {
+        // ----------------------------- producer warp ------------------------------------
+        if (lane == 0) {
+            const uint64_t pol = policy_evict_first();
+            uint32_t k = 0;
+            for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {
+                const uint32_t s = k % S;
+                if (!mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) break;
+                const uint32_t fb = smem_addr(&full_bar[s]);
+                mbar_arrive_expect_tx(fb, kStage);
+                const uint32_t dst = ring + s * kStage;
+#pragma unroll
+                for (int c = 0; c < T::kCols; ++c) {
+                    const uint32_t bytes = R * col_bits<L>(c) / 8u;
+                    bulk_g2s(dst + col_offset<L>(c, R), prm.col[c] + t * (uint64_t)bytes, bytes, fb, pol);
+                }
+            }
+            // Never leave with copies in flight: wait for the last tiles issued to land.
+            for (uint32_t i = (k > S ? k - S : 0u); i < k; ++i) mbar_wait(smem_addr(&full_bar[i % S]), (i / S) & 1u, prm.status);
+        }
+    } else {
+        // ----------------------------- consumer warps -----------------------------------
+        using Acc = typename AccSel<P, G, T::kWideQty>::T;
+        const uint32_t ctid = threadIdx.x;  // 0 .. 32W-1
+        Acc acc;
+        acc.init(lane, ctid, smem + S * kStage);
+        uint32_t bad = 0;
+        constexpr uint32_t kSteps = R / T::kRowsPerStep;  // steps per tile
+        // Rows one consumer thread adds per tile, and how often the 16-bit packed partials
+        // (quantity <= 255 per row) must be folded into 64 bits: at most every 257 rows.
+        constexpr uint32_t kTablesPerWarp = 32u / G;
+        constexpr uint32_t kRowsPerThreadTile =
+            (P == kPlaceInRegisters) ? (kSteps + W * kTablesPerWarp - 1) / (W * kTablesPerWarp) * T::kRowsPerStep
+                                     : kSteps / (W * 32) * T::kRowsPerStep;
+        constexpr uint32_t kFoldEvery = (257u / kRowsPerThreadTile) > 0 ? (257u / kRowsPerThreadTile) : 1u;
+        static_assert(kRowsPerThreadTile <= 257u, "tile too large for the packed partials");
+        static_assert(kSteps % (W * 32) == 0, "steps must divide evenly among consumer threads");
+        bool ok = true;
+        uint32_t k = 0;
+        for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {
+            const uint32_t s = k % S;
+            // Every lane waits (acquiring the bulk-copy writes); the warp proceeds only together.
+            const bool landed = mbar_wait(smem_addr(&full_bar[s]), (k / S) & 1u, prm.status);
+            if (!__all_sync(0xffffffffu, landed)) {
+                ok = false;
+                break;
+            }
+            const uint32_t base = ring + s * kStage;
+            if constexpr (P == kPlaceInRegisters) {
+                const uint32_t tbl = lane / G;
+                if (tbl < kTablesPerWarp) {
+                    for (uint32_t j = warp * kTablesPerWarp + tbl; j < kSteps; j += W * kTablesPerWarp)
+                        process_step<L>(base, j, prm.cutoff, acc, bad);
+                }
+            } else {
+#pragma unroll
+                for (uint32_t it = 0; it < kSteps / (W * 32); ++it)
+                    process_step<L>(base, ctid + it * (W * 32), prm.cutoff, acc, bad);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
+            acc.tile_done(prm, lane);
+            if ((k + 1) % kFoldEvery == 0) acc.fold();
+        }
+        acc.fold();
+        // Tail rows [num_tiles * R, rows): handled by the CTA next in the round robin.
+        if (ok && blockIdx.x == (uint32_t)(num_tiles % gridDim.x)) {
+            const uint64_t first = num_tiles * R;
+            if constexpr (P == kPlaceInRegisters) {
+                const uint32_t tbl = lane / G;
+                if (tbl < kTablesPerWarp) {
+                    for (uint64_t i = first + warp * kTablesPerWarp + tbl; i < prm.rows; i += W * kTablesPerWarp)
+                        process_row_global<L>(prm, i, acc, bad);
+                }
+            } else {
+                for (uint64_t i = first + ctid; i < prm.rows; i += W * 32) process_row_global<L>(prm, i, acc, bad);
+            }
+            acc.tile_done(prm, lane);
+        }
+        if (bad && prm.status) atomicOr(prm.status, kStatusDomain);
+        acc.flush(CtaRed{red}, lane);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < (uint32_t)(G * kNumAggs); i += blockDim.x) {
+        const uint32_t code = i / kNumAggs, agg = i % kNumAggs;
+        const uint32_t grp = (G == 4) ? prm.pair_group[code] : code;
+        uint64_t lo = red[2 * i], hi = red[2 * i + 1];
+        if (agg == kAggQty && prm.qty_scale != 1u) {
+            // 128 x 32 -> 128 multiply (sum of quantity in whole units -> hundredths)
+            const uint64_t l_lo = (lo & 0xFFFFFFFFull) * prm.qty_scale;
+            const uint64_t l_hi = (lo >> 32) * prm.qty_scale;
+            const uint64_t nlo = l_lo + (l_hi << 32);
+            hi = hi * prm.qty_scale + (l_hi >> 32) + (nlo < l_lo ? 1u : 0u);
+            lo = nlo;
+        }
+        atomic_add_u128(prm.out + 2 * (grp * kNumAggs + agg), lo, hi);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host launch table
+// ---------------------------------------------------------------------------------------------
+
+template <int L, int P>
+static cudaError_t launch_one(const ScanParams& prm, int sm_count, int max_blocks, cudaStream_t stream) {
+    constexpr uint32_t R = kTileRows<L>;
+    constexpr uint32_t S = kStages<L, P>;
+    constexpr uint32_t W = kConsumerWarps;
+    constexpr int G = LayoutTraits<L>::kCodes;
+    uint32_t dyn = S * stage_bytes<L>(R);
+    if (P == kPlaceSharedMemPerThread) dyn += (uint32_t)(44 * G * W * 32);
+    cudaError_t e = cudaFuncSetAttribute(q1_scan_kernel<L, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+    const uint64_t tiles = prm.rows / R;
+    uint64_t blocks = tiles ? tiles : 1;
+    uint64_t cap = (uint64_t)sm_count;  // one CTA per SM (shared-memory bound)
+    if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
+    if (blocks > cap) blocks = cap;
+    q1_scan_kernel<L, P><<<(unsigned)blocks, (W + 1) * 32, dyn, stream>>>(prm);
+    return cudaGetLastError();
+}
+
+template <int L>
+static cudaError_t launch_layout(int placement, const ScanParams& prm, int sm_count, int max_blocks, cudaStream_t st) {
+    switch (placement) {
+        case kPlaceInRegisters: return launch_one<L, kPlaceInRegisters>(prm, sm_count, max_blocks, st);
+        case kPlaceInRegistersPerThread: return launch_one<L, kPlaceInRegistersPerThread>(prm, sm_count, max_blocks, st);
+        case kPlaceLocalMem: return launch_one<L, kPlaceLocalMem>(prm, sm_count, max_blocks, st);
+        case kPlaceSharedMemPerThread: return launch_one<L, kPlaceSharedMemPerThread>(prm, sm_count, max_blocks, st);
+        case kPlaceGlobal: return launch_one<L, kPlaceGlobal>(prm, sm_count, max_blocks, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm_count, int max_blocks,
+                        cudaStream_t stream) {
+    switch (layout) {
+        case kLayPair: return launch_layout<kLayPair>(placement, prm, sm_count, max_blocks, stream);
+        case kLayPairFilter: return launch_layout<kLayPairFilter>(placement, prm, sm_count, max_blocks, stream);
+        case kLaySep: return launch_layout<kLaySep>(placement, prm, sm_count, max_blocks, stream);
+        case kLaySepFilter: return launch_layout<kLaySepFilter>(placement, prm, sm_count, max_blocks, stream);
+        case kLayUncomp: return launch_layout<kLayUncomp>(placement, prm, sm_count, max_blocks, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+uint32_t scan_tile_rows(int layout) {
+    switch (layout) {
+        case kLayUncomp: return kTileRows<kLayUncomp>;
+        default: return kTileRows<kLayPair>;
+    }
+}
+
+}  // namespace q1

@@ -1,0 +1,205 @@
+// tpch_01 -- drop-in command line of the reference's tpch_01 (src/main.cu:738-916) over the C ABI.
+//
+// Same flags as the reference's parse_command_line (src/main.cu:255-360), in both the code
+// spelling and the README spelling (README.md:47-58): --apply-compression,
+// --use-filter-pushdown, --use-coprocessing, --print-results, --device,
+// --hash-table-placement=, --scale-factor= | --sf=, --streams=, --threads-per-block=,
+// --tuples-per-thread= | --tuples_per_thread=, --tuples-per-kernel-launch= | --tuples-per-kernel=,
+// --runs=, --cpu-fraction=.
+// Additions: --rows=N (exact row count), --seed=S (generator seed), --cutoff-day=D,
+// --resident (keep the table in HBM instead of streaming it from pinned host memory every run,
+// which is what the reference does).
+// The table comes from the seeded synthetic generator (dbgen's lineitem.tbl is not available);
+// rows = scale factor x 6,001,215 (src/constants.hpp:49). Per-run wall times go to results.csv
+// (src/main.cu:881-905).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "q1.h"
+
+static void print_help(const char* argv0) {
+    fprintf(stderr, "Unrecognized command line option.\n");
+    fprintf(stderr, "Usage: %s [args]\n", argv0);
+    fprintf(stderr, "   --apply-compression\n");
+    fprintf(stderr, "   --print-results\n");
+    fprintf(stderr, "   --use-filter-pushdown\n");
+    fprintf(stderr, "   --use-coprocessing\n");
+    fprintf(stderr, "   --hash-table-placement=[default:in_registers_per_thread]\n"
+                    "     (one of: in_registers, in_registers_per_thread, local_mem, shared_mem_per_thread, global;\n"
+                    "      or in-registers, local-mem, per-thread-shared-mem)\n");
+    fprintf(stderr, "   --runs=[default:5]\n");
+    fprintf(stderr, "   --sf=[default:1.0] | --scale-factor=   --rows=N\n");
+    fprintf(stderr, "   --cpu-fraction=[default:0.5]\n");
+    fprintf(stderr, "   --streams=[default:4]\n");
+    fprintf(stderr, "   --threads-per-block=[multiple of 32]\n");
+    fprintf(stderr, "   --tuples-per-thread=\n");
+    fprintf(stderr, "   --tuples-per-kernel-launch=[default:2097152] | --tuples-per-kernel=\n");
+    fprintf(stderr, "   --resident   --seed=S   --cutoff-day=D   --device\n");
+}
+
+static void print_device() {
+    char buf[512];
+    if (q1_device_describe(0, buf, sizeof(buf)) != Q1_OK) {
+        fprintf(stderr, "%s\n", q1_last_error());
+        return;
+    }
+    printf("%s\n", buf);
+}
+
+static void print_dec(const q1_i128& v, int64_t scale, int width) {
+    __int128 x = (__int128)(((unsigned __int128)v.hi << 64) | v.lo);
+    const bool neg = x < 0;
+    if (neg) x = -x;
+    const __int128 ip = x / scale, fp = x % scale;
+    char buf[64];
+    int n = 0;
+    __int128 t = ip;
+    char digits[48];
+    do {
+        digits[n++] = (char)('0' + (int)(t % 10));
+        t /= 10;
+    } while (t);
+    int k = 0;
+    if (neg) buf[k++] = '-';
+    while (n) buf[k++] = digits[--n];
+    buf[k] = 0;
+    int fd = 0;
+    for (int64_t s = scale; s > 1; s /= 10) ++fd;
+    printf(" | %*s.%0*lld", width - fd - 1, buf, fd, (long long)fp);
+}
+
+static void print_results(const q1_result& r) {
+    printf("+---------------------------------------------------- Results ------------------------------------------------------+\n");
+    printf("|  LS | RF |  sum_quantity        |  sum_base_price      |  sum_disc_price      |  sum_charge          | count      |\n");
+    printf("+-------------------------------------------------------------------------------------------------------------------+\n");
+    uint64_t total = 0;
+    for (uint32_t g = 0; g < r.num_groups; ++g) {
+        const q1_group_result& x = r.groups[g];
+        if (!x.count) continue;
+        printf("| # %c | %c ", x.returnflag, x.linestatus);
+        print_dec(x.sum_qty, 100, 20);
+        print_dec(x.sum_base_price, 100, 20);
+        print_dec(x.sum_disc_price, 10000, 20);
+        print_dec(x.sum_charge, 1000000, 20);
+        printf(" | %10llu |", (unsigned long long)x.count);
+        printf("  avg_qty %lld.%04lld avg_price %lld.%04lld avg_disc %lld.%04lld\n", (long long)(x.avg_qty_e4 / 10000),
+               (long long)llabs(x.avg_qty_e4 % 10000), (long long)(x.avg_price_e4 / 10000),
+               (long long)llabs(x.avg_price_e4 % 10000), (long long)(x.avg_disc_e4 / 10000),
+               (long long)llabs(x.avg_disc_e4 % 10000));
+        total += x.count;
+    }
+    printf("+-------------------------------------------------------------------------------------------------------------------+\n");
+    printf("Total number of elements tuples satisfying the WHERE clause: %llu / %llu = %f\n", (unsigned long long)total,
+           (unsigned long long)r.rows_total, r.rows_total ? (double)total / (double)r.rows_total : 0.0);
+}
+
+static bool starts(const std::string& s, const char* p) { return s.rfind(p, 0) == 0; }
+
+int main(int argc, char** argv) {
+    q1_params p;
+    q1_params_default(&p);
+    double scale_factor = 1.0;
+    uint64_t rows = 0;
+    uint64_t seed = 20260101;
+    bool print = false, resident = false;
+    for (int i = 1; i < argc; ++i) {
+        std::string a(argv[i]);
+        if (!starts(a, "--")) {
+            print_help(argv[0]);
+            return EXIT_FAILURE;
+        }
+        a = a.substr(2);
+        const size_t eq = a.find('=');
+        std::string name = eq == std::string::npos ? a : a.substr(0, eq);
+        const std::string val = eq == std::string::npos ? "" : a.substr(eq + 1);
+        for (auto& ch : name)
+            if (ch == '_') ch = '-';
+        try {
+            if (name == "device") {
+                print_device();
+                return 1;   // the reference exits after printing the device (src/main.cu:266-268)
+            } else if (name == "use-coprocessing") p.use_coprocessing = 1;
+            else if (name == "apply-compression") p.apply_compression = 1;
+            else if (name == "use-filter-pushdown") p.use_filter_pushdown = 1;
+            else if (name == "print-results") print = true;
+            else if (name == "resident") resident = true;
+            else if (name == "scale-factor" || name == "sf") {
+                scale_factor = std::stod(val);
+                if (scale_factor < 0.001) {
+                    fprintf(stderr, "Invalid scale factor %f\n", scale_factor);
+                    return EXIT_FAILURE;
+                }
+            } else if (name == "rows") rows = std::stoull(val);
+            else if (name == "seed") seed = std::stoull(val);
+            else if (name == "cutoff-day") p.cutoff_day = std::stoi(val);
+            else if (name == "hash-table-placement") {
+                q1_placement pl;
+                if (q1_placement_from_name(val.c_str(), &pl) != Q1_OK) {
+                    fprintf(stderr, "%s\n", q1_last_error());
+                    return EXIT_FAILURE;
+                }
+                p.placement = pl;
+            } else if (name == "streams") p.streams = std::stoi(val);
+            else if (name == "tuples-per-thread") p.tuples_per_thread = std::stoi(val);
+            else if (name == "threads-per-block") p.threads_per_block = std::stoi(val);
+            else if (name == "tuples-per-kernel-launch" || name == "tuples-per-kernel") p.tuples_per_launch = std::stoll(val);
+            else if (name == "runs") p.runs = std::stoi(val);
+            else if (name == "cpu-fraction") p.cpu_fraction = std::stod(val);
+            else {
+                print_help(argv[0]);
+                return EXIT_FAILURE;
+            }
+        } catch (const std::exception&) {
+            fprintf(stderr, "Cannot parse the value passed after --%s=\n", name.c_str());
+            return EXIT_FAILURE;
+        }
+    }
+    if (q1_params_validate(&p) != Q1_OK) {
+        fprintf(stderr, "%s\n", q1_last_error());
+        return EXIT_FAILURE;
+    }
+    if (!rows) rows = (uint64_t)(scale_factor * 6001215.0);
+
+    q1_ctx* ctx = nullptr;
+    q1_device_opts opts{0, 0};
+    if (q1_open(&ctx, &opts) != Q1_OK) {
+        fprintf(stderr, "q1_open: %s\n", q1_last_error());
+        return EXIT_FAILURE;
+    }
+    const q1_residency res = resident ? Q1_RESIDENCY_HBM : Q1_RESIDENCY_PINNED_HOST;
+    printf("Generating %llu lineitem rows (seed %llu, %s, %s)... ", (unsigned long long)rows,
+           (unsigned long long)seed, p.apply_compression ? "compressed" : "uncompressed",
+           resident ? "HBM-resident" : "pinned host memory, streamed each run");
+    fflush(stdout);
+    q1_status st = q1_generate_table(ctx, seed, 0, rows, p.apply_compression ? Q1_LAYOUT_COMPRESSED : Q1_LAYOUT_UNCOMPRESSED,
+                                     Q1_FLAGS_PAIR_2BIT, res);
+    if (st != Q1_OK) {
+        fprintf(stderr, "\ntable generation failed: %s\n", q1_last_error());
+        q1_close(ctx);
+        return EXIT_FAILURE;
+    }
+    printf("done.\n");
+    std::ofstream csv("results.csv", std::ios::out);
+    const int runs = p.runs;
+    p.runs = 1;
+    q1_result r;
+    for (int run = 0; run < runs; ++run) {
+        printf("Executing TPC-H Query 1, run %d of %d... ", run + 1, runs);
+        fflush(stdout);
+        st = q1_run(ctx, &p, &r);
+        if (st != Q1_OK) {
+            fprintf(stderr, "\nq1_run: %s: %s\n", q1_status_string(st), q1_last_error());
+            q1_close(ctx);
+            return EXIT_FAILURE;
+        }
+        printf("done.\n");
+        csv << r.ms_last_run / 1000.0 << '\n';
+        if (print) print_results(r);
+    }
+    q1_close(ctx);
+    return 0;
+}
