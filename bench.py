@@ -177,7 +177,7 @@ def reference_arm(args, rank):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": config_dict(args.gpus, "cpu"),
+            "data": "synthetic", "config": config_dict(args.gpus, args.placement),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -185,6 +185,7 @@ def reference_arm(args, rank):
 
 
 def main():
+    global ROWS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -195,7 +196,6 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
-    global ROWS
     ROWS = args.rows
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
