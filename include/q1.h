@@ -308,6 +308,23 @@ q1_status q1_launch_compressed(q1_placement placement, const q1_compressed_colum
                                const q1_launch_config* cfg, q1_i128* dev_aggregates,
                                void* cuda_stream);
 
+/* Allocation-free variant of q1_launch_compressed (no counterpart in the reference).
+ * For callers that must not allocate device memory: a host that owns every byte of device
+ * memory through its own pool or runs under a hard memory cap, or a latency-critical loop in
+ * which cudaMalloc/cudaFree must never run. q1_launch_compressed allocates a small status word on
+ * first use of a device; this call allocates nothing. Its scratch is a static device array of
+ * 147,712 bytes that every GPU loading the library holds until exit: a status word plus one
+ * partial-sum record per CTA, which a second kernel adds into dev_aggregates (accumulating, like
+ * q1_launch_compressed). Limit: at most 256 CTAs per launch (one per SM is used by default, 148
+ * on a B200); larger grids are rejected with Q1_ERR_INVALID_ARGUMENT. The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress). The call is synchronous: it waits for
+ * `cuda_stream` and returns Q1_ERR_DOMAIN / Q1_ERR_DEVICE_TIMEOUT itself. All calls share the
+ * array, so calls whose GPU work overlaps (other threads or streams of the same device) race. */
+q1_status q1_launch_compressed_noalloc(q1_placement placement, const q1_compressed_columns* dev_cols,
+                                       uint64_t rows, int32_t cutoff_day, int32_t use_filter,
+                                       const q1_launch_config* cfg, q1_i128* dev_aggregates,
+                                       void* cuda_stream);
+
 /* Replaces the kernels table (src/main.cu:166-173): K1, K4, K7, K10, K13. */
 q1_status q1_launch_uncompressed(q1_placement placement, const q1_columns* dev_cols,
                                  uint64_t rows, int32_t cutoff_day,

@@ -129,6 +129,9 @@ SIGNATURES = {
                                             ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(LaunchConfig), vp, vp]),
     "q1_launch_uncompressed": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Columns), ctypes.c_uint64, ctypes.c_int32,
                                               ctypes.POINTER(LaunchConfig), vp, vp]),
+    "q1_launch_compressed_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(CompressedColumns), ctypes.c_uint64,
+                                                    ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(LaunchConfig), vp,
+                                                    vp]),
     "q1_sync_check": (ctypes.c_int, [vp]),
     "q1_precompute_filter": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int32, vp, vp]),
     "q1_generate_host": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(Columns)]),

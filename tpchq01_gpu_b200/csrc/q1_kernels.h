@@ -43,12 +43,17 @@ struct ScanParams {
     uint8_t pair_group[4];      // pair layouts: code -> group
     unsigned long long* out;    // [6 groups][6 aggregates][lo, hi]
     uint32_t* status;           // device status word (kStatus* bits); may be null
+    unsigned long long* records;  // null: atomics into `out`. Otherwise each CTA writes its own
+                                  // [6][6][lo, hi] record at records[blockIdx.x] and leaves `out`
+                                  // alone (used by the allocation-free entry point)
 };
 
 // Launch the scan kernel for one layout x placement. max_blocks <= 0: one CTA per SM.
 cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm_count, int max_blocks,
                         cudaStream_t stream);
 uint32_t scan_tile_rows(int layout);
+// Grid size launch_scan uses for `rows` rows of `layout`.
+uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks);
 
 // Utility kernels (util_kernels.cu).
 struct GenCompressedOut {

@@ -586,6 +586,30 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
         acc.flush(CtaRed{red}, lane);
     }
     __syncthreads();
+    if (prm.records) {
+        // Per-CTA record instead of atomics: one thread per (group, aggregate), summing the codes
+        // that map to the group.
+        unsigned long long* rec = prm.records + (uint64_t)blockIdx.x * (kNumGroups * kNumAggs * 2);
+        for (uint32_t i = threadIdx.x; i < (uint32_t)(kNumGroups * kNumAggs); i += blockDim.x) {
+            const uint32_t grp = i / kNumAggs, agg = i % kNumAggs;
+            uint64_t lo = 0, hi = 0;
+            for (uint32_t code = 0; code < (uint32_t)G; ++code) {
+                if (((G == 4) ? prm.pair_group[code] : code) != grp) continue;
+                uint64_t clo = red[2 * (code * kNumAggs + agg)], chi = red[2 * (code * kNumAggs + agg) + 1];
+                if (agg == kAggQty && prm.qty_scale != 1u) {
+                    const unsigned __int128 v = ((unsigned __int128)chi << 64 | clo) * prm.qty_scale;
+                    clo = (uint64_t)v;
+                    chi = (uint64_t)(v >> 64);
+                }
+                const uint64_t nlo = lo + clo;
+                hi += chi + (nlo < lo ? 1u : 0u);
+                lo = nlo;
+            }
+            rec[2 * i] = lo;
+            rec[2 * i + 1] = hi;
+        }
+        return;
+    }
     for (uint32_t i = threadIdx.x; i < (uint32_t)(G * kNumAggs); i += blockDim.x) {
         const uint32_t code = i / kNumAggs, agg = i % kNumAggs;
         const uint32_t grp = (G == 4) ? prm.pair_group[code] : code;
@@ -616,12 +640,8 @@ static cudaError_t launch_one(const ScanParams& prm, int sm_count, int max_block
     if (P == kPlaceSharedMemPerThread) dyn += (uint32_t)(44 * G * W * 32);
     cudaError_t e = cudaFuncSetAttribute(q1_scan_kernel<L, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
-    const uint64_t tiles = prm.rows / R;
-    uint64_t blocks = tiles ? tiles : 1;
-    uint64_t cap = (uint64_t)sm_count;  // one CTA per SM (shared-memory bound)
-    if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
-    if (blocks > cap) blocks = cap;
-    q1_scan_kernel<L, P><<<(unsigned)blocks, (W + 1) * 32, dyn, stream>>>(prm);
+    const uint32_t blocks = scan_grid_blocks(L, prm.rows, sm_count, max_blocks);
+    q1_scan_kernel<L, P><<<blocks, (W + 1) * 32, dyn, stream>>>(prm);
     return cudaGetLastError();
 }
 
@@ -647,6 +667,15 @@ cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm
         case kLayUncomp: return launch_layout<kLayUncomp>(placement, prm, sm_count, max_blocks, stream);
         default: return cudaErrorInvalidValue;
     }
+}
+
+uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks) {
+    const uint64_t tiles = rows / scan_tile_rows(layout);
+    uint64_t blocks = tiles ? tiles : 1;
+    uint64_t cap = (uint64_t)sm_count;  // one CTA per SM (shared-memory bound)
+    if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
+    if (blocks > cap) blocks = cap;
+    return (uint32_t)blocks;
 }
 
 uint32_t scan_tile_rows(int layout) {
