@@ -121,7 +121,7 @@ typedef struct q1_columns {
  * Bit containers are uint32 words, element i at word i/(32/b), bit b*(i%(32/b)), LSB first
  * (src/bit_operations.hpp:60-154). */
 typedef struct q1_compressed_columns {
-    const uint16_t* shipdate;      /* day - 727563                                              */
+    const uint16_t* shipdate;      /* day - 727563, at most 32767 (dates up to 2081-09-19)      */
     const uint8_t*  discount;      /* hundredths, 0..100                                        */
     const uint32_t* extendedprice; /* cents                                                     */
     const uint8_t*  tax;           /* hundredths                                                */
@@ -335,6 +335,37 @@ q1_status q1_launch_uncompressed(q1_placement placement, const q1_columns* dev_c
  * current device's kernel status word (bounded-wait expiry, out-of-domain rows) into a status
  * code, clearing it. Replaces the reference's reliance on cuda-api-wrappers exceptions. */
 q1_status q1_sync_check(void* cuda_stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Group-key aggregation: the same predicate and aggregates, grouped by a uint32 key column     */
+/* (key < num_groups <= Q1_MAX_KEY_GROUPS) instead of (returnflag, linestatus). Generalises the  */
+/* reference's 6-entry group table (src/constants.hpp:56) to many groups.                      */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Bytes of device scratch q1_launch_groupkey needs for num_groups groups. */
+uint64_t q1_groupkey_scratch_bytes(uint32_t num_groups);
+
+/* Placements: IN_REGISTERS_PER_THREAD (num_groups <= 8), SHARED_MEM_PER_THREAD (a per-CTA
+ * shared-memory table for keys < 2048, larger keys spilled to global atomics), GLOBAL (global
+ * atomics for every row). Reads ship, qty, disc, tax, price of dev_cols and dev_keys; the result
+ * accumulates into dev_aggregates[num_groups][6] (caller-zeroed int128). dev_scratch: device
+ * memory of q1_groupkey_scratch_bytes(num_groups), owned by the caller; calls on different
+ * streams need different scratch. A key >= num_groups in a passing row is reported as
+ * Q1_ERR_DOMAIN by q1_sync_check. */
+q1_status q1_launch_groupkey(q1_placement placement, const q1_compressed_columns* dev_cols,
+                             const uint32_t* dev_keys, uint32_t num_groups, uint64_t rows,
+                             int32_t cutoff_day, const q1_launch_config* cfg, void* dev_scratch,
+                             q1_i128* dev_aggregates, void* cuda_stream);
+
+/* Zipf(s) inverse-CDF thresholds over ranks 1..num_groups (key = rank - 1): cdf[k] =
+ * floor(2^32 * P(rank <= k+1)), clamped to 0xFFFFFFFF, last entry 0xFFFFFFFF. */
+q1_status q1_zipf_cdf(uint32_t num_groups, double s, uint32_t* cdf_out);
+
+/* Group keys of the seeded generator for rows [first_row, first_row+rows): uniform over
+ * [0, num_groups) if dev_cdf is NULL, else the smallest k with bits <= dev_cdf[k]. */
+q1_status q1_generate_group_keys_device(uint64_t seed, uint64_t first_row, uint64_t rows,
+                                        uint32_t num_groups, const uint32_t* dev_cdf,
+                                        uint32_t* dev_keys, void* cuda_stream);
 
 /* Device filter precomputation (GPU version of src/main.cu:362-389). */
 q1_status q1_precompute_filter(const uint16_t* dev_shipdate, uint64_t rows, int32_t cutoff_day,

@@ -1,0 +1,123 @@
+"""Group-key aggregation (uint32 key, up to 65,536 groups) against the oracle: every placement,
+group counts 4 / 64 / 1024 / 65536, uniform and Zipf(1.1) keys, cutoffs from ~1% to 100% passing.
+Integer results, tolerance 0."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import gen_np
+import tpchq01_gpu_b200 as q
+from oracle import py_oracle as O
+from tpchq01_gpu_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+ROWS = 400_037
+SEED = 555
+
+
+def zipf_cdf(g, s=1.1):
+    cdf = np.zeros(g, dtype=np.uint32)
+    _lib.check(q.lib().q1_zipf_cdf(g, s, cdf.ctypes.data_as(ctypes.c_void_p)))
+    return cdf
+
+
+@pytest.fixture(scope="module")
+def table(cuda):
+    cols = gen_np.generate(SEED, 0, ROWS)
+    comp = gen_np.compress(cols)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).copy()).cuda()
+           for k, v in comp.items() if isinstance(v, np.ndarray) and k != "pair_group"}
+    c = _lib.CompressedColumns()
+    for k in ["shipdate", "discount", "extendedprice", "tax", "quantity"]:
+        setattr(c, k, dev[k].data_ptr())
+    return comp, c, dev
+
+
+def keys_for(num_groups, dist):
+    if dist == "uniform":
+        return gen_np.group_keys_uniform(SEED, 0, ROWS, num_groups), None
+    cdf = zipf_cdf(num_groups)
+    return gen_np.group_keys_cdf(SEED, 0, ROWS, cdf), cdf
+
+
+def run_gpu(c, keys, num_groups, placement, cutoff):
+    dkeys = torch.from_numpy(keys.view(np.int32).copy()).cuda()
+    scratch = torch.zeros(int(q.lib().q1_groupkey_scratch_bytes(num_groups)) // 8 + 2, dtype=torch.int64, device="cuda")
+    out = torch.zeros(num_groups * 12, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    cfg = _lib.LaunchConfig(0, 0, 0)
+    _lib.check(q.lib().q1_launch_groupkey(q.placement_id(placement), ctypes.byref(c), ctypes.c_void_p(dkeys.data_ptr()),
+                                          num_groups, ROWS, cutoff, ctypes.byref(cfg),
+                                          ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                          ctypes.c_void_p(stream)))
+    _lib.check(q.lib().q1_sync_check(ctypes.c_void_p(stream)))
+    torch.cuda.synchronize()
+    return out.cpu().numpy().view(np.uint64)
+
+
+def check(comp, keys, num_groups, cutoff, got):
+    want, flag = O.q1_groupkey(comp, keys, num_groups, cutoff)
+    assert flag == 0
+    assert np.array_equal(got, want), "group-key aggregates differ from the oracle"
+
+
+# cutoffs: 1995-01-01-ish (~43%), 1998-09-02 (~98%), everything, ~1%
+CUTOFFS = [727600, 728660, 729999, 730089]
+
+
+@pytest.mark.parametrize("num_groups", [4, 64, 1024, 65536])
+@pytest.mark.parametrize("dist", ["uniform", "zipf"])
+@pytest.mark.parametrize("placement", ["shared_mem_per_thread", "global"])
+def test_groupkey_placements(table, num_groups, dist, placement):
+    comp, c, _ = table
+    keys, _ = keys_for(num_groups, dist)
+    for cutoff in [729999, 727600]:
+        check(comp, keys, num_groups, cutoff, run_gpu(c, keys, num_groups, placement, cutoff))
+
+
+@pytest.mark.parametrize("num_groups", [1, 4, 8])
+@pytest.mark.parametrize("cutoff", CUTOFFS)
+def test_groupkey_registers(table, num_groups, cutoff):
+    comp, c, _ = table
+    keys, _ = keys_for(num_groups, "uniform")
+    check(comp, keys, num_groups, cutoff, run_gpu(c, keys, num_groups, "in_registers_per_thread", cutoff))
+
+
+def test_registers_refuse_many_groups(table):
+    comp, c, _ = table
+    keys, _ = keys_for(64, "uniform")
+    with pytest.raises(q.Q1Error) as e:
+        run_gpu(c, keys, 64, "in_registers_per_thread", 729999)
+    assert e.value.status == 5
+
+
+def test_key_out_of_range_is_reported(table):
+    comp, c, _ = table
+    keys, _ = keys_for(64, "uniform")
+    keys = keys.copy()
+    keys[100] = 64
+    with pytest.raises(q.Q1Error) as e:
+        run_gpu(c, keys, 64, "global", 730089)
+    assert e.value.status == 6
+
+
+@pytest.mark.parametrize("num_groups,dist", [(1024, "uniform"), (65536, "zipf")])
+def test_device_key_generator(cuda, num_groups, dist):
+    keys, cdf = keys_for(num_groups, dist)
+    out = torch.zeros(ROWS, dtype=torch.int32, device="cuda")
+    dcdf = None if cdf is None else torch.from_numpy(cdf.view(np.int32).copy()).cuda()
+    _lib.check(q.lib().q1_generate_group_keys_device(SEED, 0, ROWS, num_groups,
+                                                     None if dcdf is None else ctypes.c_void_p(dcdf.data_ptr()),
+                                                     ctypes.c_void_p(out.data_ptr()), None))
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), keys)
+
+
+def test_zipf_cdf_matches_restatement():
+    cdf = zipf_cdf(65536)
+    ref = gen_np.zipf_cdf(65536)
+    assert cdf[-1] == 0xFFFFFFFF and np.all(np.diff(cdf.astype(np.int64)) >= 0)
+    assert np.max(np.abs(cdf.astype(np.int64) - ref.astype(np.int64))) <= 1

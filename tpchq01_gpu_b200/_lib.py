@@ -133,6 +133,12 @@ SIGNATURES = {
                                                     ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(LaunchConfig), vp,
                                                     vp]),
     "q1_sync_check": (ctypes.c_int, [vp]),
+    "q1_groupkey_scratch_bytes": (ctypes.c_uint64, [ctypes.c_uint32]),
+    "q1_launch_groupkey": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(CompressedColumns), vp, ctypes.c_uint32,
+                                          ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(LaunchConfig), vp, vp, vp]),
+    "q1_zipf_cdf": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_double, vp]),
+    "q1_generate_group_keys_device": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                                     ctypes.c_uint32, vp, vp, vp]),
     "q1_precompute_filter": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int32, vp, vp]),
     "q1_generate_host": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(Columns)]),
     "q1_generate_compressed_device": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,

@@ -120,8 +120,8 @@ extern "C" q1_status q1_launch_compressed_noalloc(q1_placement placement, const 
             max_blocks = (int)std::min<uint64_t>((rows + per - 1) / per, (uint64_t)sms);
         }
     }
-    const uint64_t kMaxRows = 1ull << 31;
-    const uint32_t grid = scan_grid_blocks(layout, std::min(rows, kMaxRows), sms, max_blocks);
+    const uint32_t grid = scan_grid_blocks(layout, rows, sms, max_blocks);
+    const uint64_t kMaxRows = scan_max_rows_per_launch(layout, placement, grid);
     if (grid > kNoAllocMaxCtas)
         return set_error(Q1_ERR_INVALID_ARGUMENT,
                          "q1_launch_compressed_noalloc: the launch needs " + std::to_string(grid) +
@@ -144,7 +144,7 @@ extern "C" q1_status q1_launch_compressed_noalloc(q1_placement placement, const 
         for (int k = 0; k < ncols; ++k) prm.col[k] = cols[k] + off * (uint64_t)bits[k] / 8;
         prm.rows = n;
         const int64_t rel = (int64_t)cutoff_day - kShipDateFrame;
-        prm.cutoff = rel < -1 ? -1 : (rel > 65535 ? 65535 : (int32_t)rel);
+        prm.cutoff = rel < -1 ? -1 : (rel > 32767 ? 32767 : (int32_t)rel);
         prm.qty_scale = 100u;
         for (int i = 0; i < 4; ++i) prm.pair_group[i] = pg[i];
         prm.out = reinterpret_cast<unsigned long long*>(dev_aggregates);

@@ -706,7 +706,7 @@ static q1_status run_once(q1_ctx* ctx, const q1_params* prm, Agg128* total, doub
     const bool pushdown = prm->use_filter_pushdown != 0;
     const bool coproc = prm->use_coprocessing != 0;
     cudaStream_t s0 = ctx->streams[0];
-    const int32_t cutoff_rel = (int32_t)std::max<int64_t>(-1, std::min<int64_t>(65535, (int64_t)prm->cutoff_day - kShipDateFrame));
+    const int32_t cutoff_rel = (int32_t)std::max<int64_t>(-1, std::min<int64_t>(32767, (int64_t)prm->cutoff_day - kShipDateFrame));
 
     // CPU/GPU split (src/main.cu:517-550): the CPU share starts at a chunk boundary.
     uint64_t cpu_start = N;

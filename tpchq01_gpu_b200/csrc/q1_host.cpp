@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -194,7 +195,7 @@ q1_status q1_compress_host(const q1_columns* in, uint64_t rows, q1_flag_packing 
                 const int64_t d = in->discount[i], x = in->tax[i], p = in->extendedprice[i], q = in->quantity[i];
                 const char rf = in->returnflag[i], ls = in->linestatus[i];
                 const char* why = nullptr;
-                if (s < 0 || s > 65535) why = "shipdate outside [1992-01-01, 1992-01-01 + 65535 days]";
+                if (s < 0 || s > 32767) why = "shipdate outside [1992-01-01, 1992-01-01 + 32767 days]";
                 else if (d < 0 || d > 100) why = "discount outside [0, 1.00]";
                 else if (x < 0 || x > 255) why = "tax outside [0, 2.55]";
                 else if (p < 0 || p > 0xFFFFFFFFll) why = "extendedprice outside uint32 cents";
@@ -385,8 +386,9 @@ static q1_status scan_launch(int layout, q1_placement placement, const uint8_t* 
         }
     }
 
-    // Launches of at most 2^31 rows (tile aligned) keep per-thread 64-bit partials exact.
-    const uint64_t kMaxRows = 1ull << 31;
+    // Launch size bound that keeps every per-thread partial exact (scan_max_rows_per_launch).
+    const uint64_t kMaxRows =
+        scan_max_rows_per_launch(layout, placement, scan_grid_blocks(layout, rows, di->sm_count, max_blocks));
     for (uint64_t off = 0; off < rows; off += kMaxRows) {
         const uint64_t n = std::min(kMaxRows, rows - off);
         ScanParams prm{};
@@ -420,10 +422,12 @@ static q1_status scan_launch(int layout, q1_placement placement, const uint8_t* 
     return Q1_OK;
 }
 
+// Cutoff relative to 1992-01-01, clamped to [-1, 32767]: compressed ship offsets are at most
+// 32767, so -1 lets no row pass and 32767 lets every row pass.
 static int32_t clamp_rel(int32_t cutoff_day) {
     const int64_t r = (int64_t)cutoff_day - kShipDateFrame;
     if (r < -1) return -1;
-    if (r > 65535) return 65535;
+    if (r > 32767) return 32767;
     return (int32_t)r;
 }
 
@@ -471,6 +475,73 @@ q1_status q1_precompute_filter(const uint16_t* dev_shipdate, uint64_t rows, int3
     if (!aligned16(dev_shipdate)) return set_error(Q1_ERR_INVALID_ARGUMENT, "shipdate must be 16-byte aligned");
     cudaError_t e = launch_precompute_filter(dev_shipdate, rows, clamp_rel(cutoff_day), dev_bitmap, (cudaStream_t)cuda_stream);
     if (e != cudaSuccess) return cuda_error(e, "filter kernel launch");
+    return Q1_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Group-key aggregation
+// ---------------------------------------------------------------------------------------------
+
+uint64_t q1_groupkey_scratch_bytes(uint32_t num_groups) { return groupkey_scratch_bytes(num_groups); }
+
+q1_status q1_launch_groupkey(q1_placement placement, const q1_compressed_columns* c, const uint32_t* dev_keys,
+                             uint32_t num_groups, uint64_t rows, int32_t cutoff_day, const q1_launch_config* cfg,
+                             void* dev_scratch, q1_i128* dev_aggregates, void* cuda_stream) {
+    if (!c || !dev_aggregates || !dev_scratch) return set_error(Q1_ERR_INVALID_ARGUMENT, "null argument");
+    if (num_groups < 1 || num_groups > Q1_MAX_KEY_GROUPS)
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "num_groups must be 1..65536");
+    if (placement == Q1_PLACEMENT_IN_REGISTERS_PER_THREAD && num_groups > 8)
+        return set_error(Q1_ERR_UNSUPPORTED, "in_registers_per_thread holds at most 8 groups per thread; use "
+                                             "shared_mem_per_thread or global");
+    if (placement != Q1_PLACEMENT_IN_REGISTERS_PER_THREAD && placement != Q1_PLACEMENT_SHARED_MEM_PER_THREAD &&
+        placement != Q1_PLACEMENT_GLOBAL)
+        return set_error(Q1_ERR_UNSUPPORTED, "group-key aggregation offers in_registers_per_thread, "
+                                             "shared_mem_per_thread and global placements");
+    const uint8_t* cols[6] = {reinterpret_cast<const uint8_t*>(c->shipdate), c->quantity, c->discount, c->tax,
+                              reinterpret_cast<const uint8_t*>(c->extendedprice),
+                              reinterpret_cast<const uint8_t*>(dev_keys)};
+    for (int k = 0; k < 6; ++k) {
+        if (!cols[k] && rows) return set_error(Q1_ERR_INVALID_ARGUMENT, "missing column");
+        if (!aligned16(cols[k])) return set_error(Q1_ERR_INVALID_ARGUMENT, "device columns must start on a 16-byte boundary");
+    }
+    if (!aligned16(dev_aggregates) || !aligned16(dev_scratch))
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "aggregates and scratch must be 16-byte aligned");
+    if (rows == 0) return Q1_OK;
+    int dev = 0;
+    Q1_CUDA(cudaGetDevice(&dev));
+    DeviceInfo* di = nullptr;
+    q1_status st = device_info(dev, &di);
+    if (st != Q1_OK) return st;
+    const int max_blocks = (cfg && cfg->blocks > 0) ? cfg->blocks : 0;
+    cudaError_t e = launch_groupkey(placement, cols, rows, clamp_rel(cutoff_day), num_groups,
+                                    reinterpret_cast<unsigned long long*>(dev_scratch),
+                                    reinterpret_cast<unsigned long long*>(dev_aggregates), di->status, di->sm_count,
+                                    max_blocks, (cudaStream_t)cuda_stream);
+    if (e != cudaSuccess) return cuda_error(e, "group-key kernel launch");
+    return Q1_OK;
+}
+
+q1_status q1_zipf_cdf(uint32_t num_groups, double s, uint32_t* cdf) {
+    if (!cdf || num_groups < 1) return set_error(Q1_ERR_INVALID_ARGUMENT, "bad argument");
+    std::vector<double> c(num_groups);
+    double acc = 0;
+    for (uint32_t k = 0; k < num_groups; ++k) {
+        acc += 1.0 / std::pow((double)(k + 1), s);
+        c[k] = acc;
+    }
+    for (uint32_t k = 0; k < num_groups; ++k) {
+        double t = std::floor(c[k] / acc * 4294967296.0);
+        cdf[k] = t >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)t;
+    }
+    cdf[num_groups - 1] = 0xFFFFFFFFu;
+    return Q1_OK;
+}
+
+q1_status q1_generate_group_keys_device(uint64_t seed, uint64_t first_row, uint64_t rows, uint32_t num_groups,
+                                        const uint32_t* dev_cdf, uint32_t* dev_keys, void* cuda_stream) {
+    if (!dev_keys || num_groups < 1) return set_error(Q1_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaError_t e = launch_generate_keys(seed, first_row, rows, num_groups, dev_cdf, dev_keys, (cudaStream_t)cuda_stream);
+    if (e != cudaSuccess) return cuda_error(e, "key generator launch");
     return Q1_OK;
 }
 

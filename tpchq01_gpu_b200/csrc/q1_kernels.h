@@ -33,7 +33,10 @@ inline constexpr uint32_t kTileRows = (L == kLayUncomp) ? 1024u : 4096u;
 template <int L, int P>
 inline constexpr uint32_t kStages = (P == kPlaceSharedMemPerThread) ? 3u : 4u;
 // Consumer warps per CTA (plus one producer warp).
-inline constexpr uint32_t kConsumerWarps = 8;
+#ifndef Q1_CONSUMER_WARPS
+#define Q1_CONSUMER_WARPS 8
+#endif
+inline constexpr uint32_t kConsumerWarps = Q1_CONSUMER_WARPS;
 
 struct ScanParams {
     const uint8_t* col[7];      // column base pointers in tile order; 16-byte aligned
@@ -54,6 +57,17 @@ cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm
 uint32_t scan_tile_rows(int layout);
 // Grid size launch_scan uses for `rows` rows of `layout`.
 uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks);
+// Most rows one launch may take so that no consumer thread adds more than 2^16 rows (which keeps
+// its 32-bit and 64-bit partial sums exact) and per-launch sums stay below 2^31 rows.
+uint64_t scan_max_rows_per_launch(int layout, int placement, uint32_t grid);
+
+// Group-key aggregation (groupkey_kernels.cu). cols: ship, qty, disc, tax, price, key.
+cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_t rows, int32_t cutoff_rel,
+                            uint32_t num_groups, unsigned long long* scratch, unsigned long long* out,
+                            uint32_t* status, int sm_count, int max_blocks, cudaStream_t stream);
+uint64_t groupkey_scratch_bytes(uint32_t num_groups);
+cudaError_t launch_generate_keys(uint64_t seed, uint64_t first_row, uint64_t rows, uint32_t num_groups,
+                                 const uint32_t* dev_cdf, uint32_t* dev_keys, cudaStream_t stream);
 
 // Utility kernels (util_kernels.cu).
 struct GenCompressedOut {

@@ -109,6 +109,14 @@ __device__ __forceinline__ uint4 lds_v4(uint32_t a) {
     return v;
 }
 
+// Byte permute with sign replication (prmt.b32, generic mode): byte n of the result is byte
+// (sel_n & 7) of {b:a}, replaced by 0x00/0xFF from that byte's top bit when sel_n & 8.
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+}
+
 // acc + a * b with a 64-bit accumulator (one wide multiply-add).
 __device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t acc) {
     uint64_t r;

@@ -156,6 +156,58 @@ struct GroupRegs {
     }
 };
 
+// Four decoded rows of a compressed tile (a "quad"), handed to a placement at once.
+struct Quad {
+    uint32_t OH;      // byte r: bit g set iff row r passes the predicate and has group code g
+    uint32_t Q, D;    // bytes r: quantity (units) and discount (hundredths) of row r
+    uint32_t a[4];    // 100 - discount
+    uint32_t ab[4];   // (100 - discount) * (100 + tax)
+    uint32_t p[4];    // extendedprice
+};
+
+// Code of row r of a quad (0..7 = group code, 7 also = filtered out) for row-wise placements.
+__device__ __forceinline__ uint32_t quad_code(const Quad& x, int r) {
+    const uint32_t b = (x.OH >> (8 * r)) & 0xFFu;
+    return b ? (uint32_t)(__ffs(b) - 1) : 7u;
+}
+
+// Aggregates of one group, per thread, fed a quad at a time. W1 (byte r = 1 iff row r is in the
+// group) drives three byte dot products (count, quantity, discount of 4 rows in one dp4a each);
+// the price products use the FMA pipe: pg = m * p (m in {0,1}), then wide multiply-adds.
+// 32-bit count/quantity/discount partials stay exact: a thread adds at most 2^16 rows per launch
+// (the host caps rows per launch at 2^16 per consumer thread), so quantity <= 255 * 2^16.
+struct GroupQuadRegs {
+    uint64_t p, dp, ch;
+    uint32_t cnt, q, d;
+    __device__ __forceinline__ void zero() {
+        p = dp = ch = 0;
+        cnt = q = d = 0;
+    }
+    __device__ __forceinline__ void add_quad(uint32_t W1, const Quad& x) {
+        cnt = __dp4a(W1, 0x01010101u, cnt);
+        q = __dp4a(W1, x.Q, q);
+        d = __dp4a(W1, x.D, d);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t m = __byte_perm(W1, 0u, 0x4440u | (uint32_t)r);
+            const uint32_t pg = m * x.p[r];
+            p += pg;
+            dp = mad_wide(x.a[r], pg, dp);
+            ch = mad_wide(x.ab[r], pg, ch);
+        }
+    }
+    __device__ __forceinline__ uint64_t value(int agg) const {
+        switch (agg) {
+            case kAggCount: return cnt;
+            case kAggQty: return q;
+            case kAggBasePrice: return p;
+            case kAggDisc: return d;
+            case kAggDiscPrice: return dp;
+            default: return ch;
+        }
+    }
+};
+
 // Shared-memory reduction target of a CTA: [codes][6] x (lo, hi).
 struct CtaRed {
     unsigned long long* v;
@@ -169,18 +221,50 @@ struct CtaRed {
 // (src/kernels/ht_in_registers_per_thread.cuh:11-79).
 template <int G, bool kWideQty>
 struct AccPerThread {
-    GroupRegs<kWideQty> g[G];
+    GroupRegs<kWideQty> g[kWideQty ? G : 1];      // row-wise path (uncompressed layout)
+    GroupQuadRegs gq[kWideQty ? 1 : G];           // quad path (compressed layouts)
     __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
 #pragma unroll
-        for (int i = 0; i < G; ++i) g[i].zero();
+        for (int i = 0; i < (kWideQty ? G : 1); ++i) g[i].zero();
+#pragma unroll
+        for (int i = 0; i < (kWideQty ? 1 : G); ++i) gq[i].zero();
     }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
+        if constexpr (kWideQty) {
 #pragma unroll
-        for (int i = 0; i < G; ++i) g[i].add(c == (uint32_t)i, q, d, a, ab, p);
+            for (int i = 0; i < G; ++i) g[i].add(c == (uint32_t)i, q, d, a, ab, p);
+        } else {
+            // one row through the quad path (tail rows)
+            Quad x;
+            x.OH = c < (uint32_t)G ? (1u << c) : 0u;
+            x.Q = q;
+            x.D = d;
+            x.a[0] = a;
+            x.ab[0] = ab;
+            x.p[0] = p;
+            x.a[1] = x.a[2] = x.a[3] = x.ab[1] = x.ab[2] = x.ab[3] = x.p[1] = x.p[2] = x.p[3] = 0;
+            add_quad(x);
+        }
+    }
+    __device__ __forceinline__ void add_quad(const Quad& x) {
+        if constexpr (!kWideQty) {
+#pragma unroll
+            for (int i = 0; i < G; ++i) gq[i].add_quad((x.OH >> i) & 0x01010101u, x);
+        }
     }
     __device__ __forceinline__ void fold() {
+        if constexpr (kWideQty) {
 #pragma unroll
-        for (int i = 0; i < G; ++i) g[i].fold();
+            for (int i = 0; i < G; ++i) g[i].fold();
+        }
+    }
+    __device__ __forceinline__ uint64_t value(int i, int a) const {
+        if constexpr (kWideQty) return g[i].value(a);
+        else return gq[i].value(a);
+    }
+    __device__ __forceinline__ void zero_group(int i) {
+        if constexpr (kWideQty) g[i].zero();
+        else gq[i].zero();
     }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
@@ -190,7 +274,7 @@ struct AccPerThread {
         for (int i = 0; i < G; ++i) {
 #pragma unroll
             for (int a = 0; a < kNumAggs; ++a) {
-                uint64_t lo = g[i].value(a), hi = 0;
+                uint64_t lo = value(i, a), hi = 0;
                 warp_sum_u128(lo, hi);
                 if (lane == 0) red.add(i, a, lo, hi);
             }
@@ -205,14 +289,29 @@ struct AccPerThread {
 template <int G, bool kWideQty>
 struct AccWarpLane {
     GroupRegs<kWideQty> r;
+    GroupQuadRegs rq;
     uint32_t my;
     __device__ __forceinline__ void init(uint32_t lane, uint32_t, uint8_t*) {
         r.zero();
+        rq.zero();
         my = lane % G;
     }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
-        r.add(c == my, q, d, a, ab, p);
+        if constexpr (kWideQty) {
+            r.add(c == my, q, d, a, ab, p);
+        } else {
+            Quad x;
+            x.OH = c == my ? 1u << my : 0u;
+            x.Q = q;
+            x.D = d;
+            x.a[0] = a;
+            x.ab[0] = ab;
+            x.p[0] = p;
+            x.a[1] = x.a[2] = x.a[3] = x.ab[1] = x.ab[2] = x.ab[3] = x.p[1] = x.p[2] = x.p[3] = 0;
+            add_quad(x);
+        }
     }
+    __device__ __forceinline__ void add_quad(const Quad& x) { rq.add_quad((x.OH >> my) & 0x01010101u, x); }
     __device__ __forceinline__ void fold() { r.fold(); }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
@@ -220,7 +319,7 @@ struct AccWarpLane {
         fold();
         if (lane < (32u / G) * G) {
 #pragma unroll
-            for (int a = 0; a < kNumAggs; ++a) red.add((int)my, a, r.value(a), 0);
+            for (int a = 0; a < kNumAggs; ++a) red.add((int)my, a, kWideQty ? r.value(a) : rq.value(a), 0);
         }
     }
 };
@@ -246,6 +345,11 @@ struct AccLocal {
             t[c][4] += d;
             cnt[c] += 1;
         }
+    }
+    __device__ __forceinline__ void add_quad(const Quad& x) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
     }
     __device__ __forceinline__ void fold() {}
     template <class P>
@@ -292,6 +396,11 @@ struct AccSharedPerThread {
             cnt[base] += 1;
         }
     }
+    __device__ __forceinline__ void add_quad(const Quad& x) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
+    }
     __device__ __forceinline__ void fold() {}
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
@@ -323,6 +432,7 @@ struct AccGlobal {
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
         buf.add(c, q, d, a, ab, p);
     }
+    __device__ __forceinline__ void add_quad(const Quad& x) { buf.add_quad(x); }
     __device__ __forceinline__ void fold() { buf.fold(); }
     template <class P>
     __device__ __forceinline__ void tile_done(const P& prm, uint32_t lane) {
@@ -332,11 +442,11 @@ struct AccGlobal {
             const int grp = G == 4 ? prm.pair_group[i] : i;
 #pragma unroll
             for (int a = 0; a < kNumAggs; ++a) {
-                uint64_t v = warp_sum_u64(buf.g[i].value(a));
+                uint64_t v = warp_sum_u64(buf.value(i, a));
                 if (a == kAggQty) v *= prm.qty_scale;
                 if (lane == (uint32_t)((i * kNumAggs + a) & 31)) atomic_add_u128(prm.out + 2 * (grp * kNumAggs + a), v, 0);
             }
-            buf.g[i].zero();
+            buf.zero_group(i);
         }
     }
     __device__ __forceinline__ void flush(CtaRed, uint32_t) {}
@@ -366,7 +476,8 @@ __device__ __forceinline__ uint32_t code_of_chars(uint32_t rf, uint32_t ls) {
 
 // One step of rows [kRowsPerStep * j, +kRowsPerStep) of the tile held at shared address `base`.
 template <int L, class Acc>
-__device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t cut, Acc& acc, uint32_t& bad) {
+__device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t cut, uint32_t lut, Acc& acc,
+                                             uint32_t& bad) {
     using T = LayoutTraits<L>;
     constexpr uint32_t R = kTileRows<L>;
     if constexpr (L == kLayUncomp) {
@@ -393,36 +504,46 @@ __device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t 
         }
     } else {
         constexpr bool kSep = (L == kLaySep || L == kLaySepFilter);
-        uint32_t passbits;
+        // pass mask of the 4 rows: byte r = 0xFF iff row r passes
+        uint32_t PM;
         if constexpr (T::kFilter) {
-            passbits = lds_u8(base + col_offset<L>(0, R) + (j >> 1)) >> ((j & 1u) * 4u);
+            const uint32_t bits = (lds_u8(base + col_offset<L>(0, R) + (j >> 1)) >> ((j & 1u) * 4u)) & 0xFu;
+            PM = ((bits * 0x00204081u) & 0x01010101u) * 0xFFu;
         } else {
+            // Two 16-bit lanes per subtraction: lane = (cut + 2^15) - ship has its top bit set iff
+            // ship <= cut; no borrow crosses lanes for ship <= 32767 and -1 <= cut <= 32767.
             const uint2 sd = lds_v2(base + col_offset<L>(0, R) + 8 * j);
-            passbits = ((int32_t)(sd.x & 0xFFFFu) <= cut ? 1u : 0u) | ((int32_t)(sd.x >> 16) <= cut ? 2u : 0u) |
-                       ((int32_t)(sd.y & 0xFFFFu) <= cut ? 4u : 0u) | ((int32_t)(sd.y >> 16) <= cut ? 8u : 0u);
+            const uint32_t c2 = (uint32_t)(cut + 32768) * 0x00010001u;
+            bad |= (sd.x | sd.y) & 0x80008000u;   // ship offset above 32767: outside the domain
+            PM = prmt(c2 - sd.x, c2 - sd.y, 0xFDB9u);
         }
-        const uint32_t Q = lds_u32(base + col_offset<L>(1, R) + 4 * j);
-        const uint32_t D = lds_u32(base + col_offset<L>(2, R) + 4 * j);
+        Quad x;
+        x.Q = lds_u32(base + col_offset<L>(1, R) + 4 * j);
+        x.D = lds_u32(base + col_offset<L>(2, R) + 4 * j);
         const uint32_t X = lds_u32(base + col_offset<L>(3, R) + 4 * j);
         const uint4 P = lds_v4(base + col_offset<L>(4, R) + 16 * j);
-        uint32_t F, LS = 0;
-        F = lds_u8(base + col_offset<L>(5, R) + j);
-        if constexpr (kSep) LS = lds_u8(base + col_offset<L>(6, R) + (j >> 1)) >> ((j & 1u) * 4u);
-        bad |= disc_out_of_domain4(D);
-        const uint32_t A = 0x64646464u - D;   // 100 - d per byte (no borrow inside the domain)
-        const uint32_t pv[4] = {P.x, P.y, P.z, P.w};
+        const uint32_t F = lds_u8(base + col_offset<L>(5, R) + j);
+        bad |= disc_out_of_domain4(x.D);
+        // one-hot group bit per row byte, from a 256-entry table indexed by the 4 codes' byte
+        uint32_t OH = lds_u32(lut + 4 * F);
+        if constexpr (kSep) {
+            // the table gives bit 2*rf; a line status of 1 doubles it to bit 2*rf+1; rf 3 -> dropped
+            const uint32_t LS = (lds_u8(base + col_offset<L>(6, R) + (j >> 1)) >> ((j & 1u) * 4u)) & 0xFu;
+            const uint32_t lsm = ((LS * 0x00204081u) & 0x01010101u) * 0xFFu;   // byte r = 0xFF iff ls_r
+            OH = (OH + (OH & lsm)) & 0x3F3F3F3Fu;
+        }
+        x.OH = OH & PM;
+        const uint32_t A = 0x64646464u - x.D;   // 100 - d per byte (no borrow inside the domain)
+        x.p[0] = P.x;
+        x.p[1] = P.y;
+        x.p[2] = P.z;
+        x.p[3] = P.w;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            uint32_t code;
-            if constexpr (kSep) code = (((F >> (2 * r)) & 3u) << 1) | ((LS >> r) & 1u);
-            else code = (F >> (2 * r)) & 3u;
-            const uint32_t c = ((passbits >> r) & 1u) ? code : 7u;
-            const uint32_t q = (Q >> (8 * r)) & 0xFFu;
-            const uint32_t d = (D >> (8 * r)) & 0xFFu;
-            const uint32_t a = (A >> (8 * r)) & 0xFFu;
-            const uint32_t t = (X >> (8 * r)) & 0xFFu;
-            acc.add(c, q, d, a, a * (100u + t), pv[r]);
+            x.a[r] = __byte_perm(A, 0u, 0x4440u | (uint32_t)r);
+            x.ab[r] = x.a[r] * (100u + __byte_perm(X, 0u, 0x4440u | (uint32_t)r));
         }
+        acc.add_quad(x);
     }
 }
 
@@ -448,7 +569,9 @@ __device__ __forceinline__ void process_row_global(const ScanParams& prm, uint64
         if constexpr (T::kFilter) {
             pass = (__ldg(reinterpret_cast<const uint32_t*>(prm.col[0]) + (i >> 5)) >> (i & 31)) & 1u;
         } else {
-            pass = (int32_t)__ldg(reinterpret_cast<const uint16_t*>(prm.col[0]) + i) <= prm.cutoff;
+            const uint32_t ship = __ldg(reinterpret_cast<const uint16_t*>(prm.col[0]) + i);
+            bad |= ship > 32767u;
+            pass = (int32_t)ship <= prm.cutoff;
         }
         const uint32_t q = __ldg(prm.col[1] + i);
         const uint32_t d = __ldg(prm.col[2] + i);
@@ -501,6 +624,17 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
         fence_mbar_init();
     }
     for (uint32_t i = threadIdx.x; i < (uint32_t)(G * kNumAggs * 2); i += blockDim.x) red[i] = 0;
+    // byte of four 2-bit codes -> one-hot bit per row byte (pair: bit code; separate: bit 2*rf)
+    __shared__ uint32_t code_lut[256];
+    for (uint32_t f = threadIdx.x; f < 256; f += blockDim.x) {
+        uint32_t v = 0;
+        for (uint32_t r = 0; r < 4; ++r) {
+            const uint32_t code = (f >> (2 * r)) & 3u;
+            v |= (1u << (G == 4 ? code : 2 * code)) << (8 * r);
+        }
+        code_lut[f] = v;
+    }
+    const uint32_t lut = smem_addr(code_lut);
     __syncthreads();
 
     if (warp == W) {
@@ -555,12 +689,12 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
                 const uint32_t tbl = lane / G;
                 if (tbl < kTablesPerWarp) {
                     for (uint32_t j = warp * kTablesPerWarp + tbl; j < kSteps; j += W * kTablesPerWarp)
-                        process_step<L>(base, j, prm.cutoff, acc, bad);
+                        process_step<L>(base, j, prm.cutoff, lut, acc, bad);
                 }
             } else {
 #pragma unroll
                 for (uint32_t it = 0; it < kSteps / (W * 32); ++it)
-                    process_step<L>(base, ctid + it * (W * 32), prm.cutoff, acc, bad);
+                    process_step<L>(base, ctid + it * (W * 32), prm.cutoff, lut, acc, bad);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
@@ -667,6 +801,16 @@ cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm
         case kLayUncomp: return launch_layout<kLayUncomp>(placement, prm, sm_count, max_blocks, stream);
         default: return cudaErrorInvalidValue;
     }
+}
+
+uint64_t scan_max_rows_per_launch(int layout, int placement, uint32_t grid) {
+    // accumulating lanes per CTA: every consumer thread, or the lanes of one warp-lane table
+    const uint64_t codes = (layout == kLayPair || layout == kLayPairFilter) ? 4 : 6;
+    const uint64_t lanes = placement == kPlaceInRegisters ? kConsumerWarps * (32 / codes) : kConsumerWarps * 32;
+    uint64_t n = (uint64_t)grid * lanes * 65536ull;
+    if (n > (1ull << 31)) n = 1ull << 31;
+    const uint64_t tile = scan_tile_rows(layout);
+    return n / tile * tile;
 }
 
 uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks) {
