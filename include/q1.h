@@ -367,6 +367,50 @@ q1_status q1_generate_group_keys_device(uint64_t seed, uint64_t first_row, uint6
                                         uint32_t num_groups, const uint32_t* dev_cdf,
                                         uint32_t* dev_keys, void* cuda_stream);
 
+/* ------------------------------------------------------------------------------------------ */
+/* Batched aggregation: many independent group-key instances (each its own table, cutoff and    */
+/* group count) in one persistent kernel over a device work queue of row tiles, replayed as a   */
+/* CUDA graph. Replaces one launch per instance (the reference launches one kernel per chunk,   */
+/* src/main.cu:567-719). Results equal q1_launch_groupkey's for every instance, bit for bit.    */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct q1_batch_instance {
+    q1_compressed_columns cols;   /* device: shipdate, discount, extendedprice, tax, quantity   */
+    const uint32_t* keys;         /* device group keys, < num_groups                            */
+    uint64_t rows;
+    int32_t  cutoff_day;
+    uint32_t num_groups;          /* 1..65536                                                   */
+    q1_i128* aggregates;          /* device [num_groups][6] result table                        */
+} q1_batch_instance;
+
+typedef struct q1_batch_opts {
+    int32_t use_graph;            /* capture one execution as a CUDA graph and replay it        */
+    int32_t accumulate;           /* 0: each run overwrites the result tables; 1: adds to them  */
+    int32_t chunk_tiles;          /* work-item size in 2048-row tiles; 0 = heuristic / tuner    */
+    int32_t tune;                 /* 0 heuristic placements; 1 autotune, reuse the cache file;
+                                     2 autotune and re-measure every class                      */
+    const char* tune_cache;       /* autotuner cache file (NULL: kept in memory only)           */
+} q1_batch_opts;
+
+typedef struct q1_batch_desc {
+    uint32_t instances, items, chunk_tiles, tile_rows, grid, uses_graph, tuned_classes;
+    uint32_t mode_count[3];       /* instances per placement: registers, shared table, global  */
+    uint64_t total_rows, total_groups;
+} q1_batch_desc;
+
+typedef struct q1_batch q1_batch;
+
+/* Build a batch (descriptors, work queue, scratch; autotuning runs here, on cuda_stream). The
+ * instance arrays must stay valid while the batch is used. */
+q1_status q1_batch_create(const q1_batch_instance* instances, uint32_t n, const q1_batch_opts* opts,
+                          void* cuda_stream, q1_batch** out);
+/* One execution of every instance (asynchronous; q1_sync_check reports device errors). */
+q1_status q1_batch_run(q1_batch* b, void* cuda_stream);
+q1_status q1_batch_describe(q1_batch* b, q1_batch_desc* out);
+/* Placement chosen for instance i: 0 registers, 1 shared table, 2 global. */
+q1_status q1_batch_instance_mode(q1_batch* b, uint32_t i, int32_t* mode);
+q1_status q1_batch_destroy(q1_batch* b);
+
 /* Device filter precomputation (GPU version of src/main.cu:362-389). */
 q1_status q1_precompute_filter(const uint16_t* dev_shipdate, uint64_t rows, int32_t cutoff_day,
                                uint32_t* dev_bitmap, void* cuda_stream);

@@ -99,6 +99,23 @@ class LaunchConfig(ctypes.Structure):
                 ("blocks", ctypes.c_int32)]
 
 
+class BatchInstance(ctypes.Structure):
+    _fields_ = [("cols", CompressedColumns), ("keys", vp), ("rows", ctypes.c_uint64), ("cutoff_day", ctypes.c_int32),
+                ("num_groups", ctypes.c_uint32), ("aggregates", vp)]
+
+
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("use_graph", ctypes.c_int32), ("accumulate", ctypes.c_int32), ("chunk_tiles", ctypes.c_int32),
+                ("tune", ctypes.c_int32), ("tune_cache", ctypes.c_char_p)]
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("instances", ctypes.c_uint32), ("items", ctypes.c_uint32), ("chunk_tiles", ctypes.c_uint32),
+                ("tile_rows", ctypes.c_uint32), ("grid", ctypes.c_uint32), ("uses_graph", ctypes.c_uint32),
+                ("tuned_classes", ctypes.c_uint32), ("mode_count", ctypes.c_uint32 * 3),
+                ("total_rows", ctypes.c_uint64), ("total_groups", ctypes.c_uint64)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/q1.h
 SIGNATURES = {
     "q1_last_error": (ctypes.c_char_p, []),
@@ -144,6 +161,12 @@ SIGNATURES = {
     "q1_generate_compressed_device": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
                                                      ctypes.POINTER(CompressedHostOut), vp]),
     "q1_device_describe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t]),
+    "q1_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchInstance), ctypes.c_uint32, ctypes.POINTER(BatchOpts), vp,
+                                       ctypes.POINTER(vp)]),
+    "q1_batch_run": (ctypes.c_int, [vp, vp]),
+    "q1_batch_describe": (ctypes.c_int, [vp, ctypes.POINTER(BatchDesc)]),
+    "q1_batch_instance_mode": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32)]),
+    "q1_batch_destroy": (ctypes.c_int, [vp]),
     "q1_version": (ctypes.c_char_p, []),
 }
 

@@ -57,7 +57,7 @@ cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm
 uint32_t scan_tile_rows(int layout);
 // Grid size launch_scan uses for `rows` rows of `layout`.
 uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks);
-// Most rows one launch may take so that no consumer thread adds more than 2^16 rows (which keeps
+// Most rows one launch may take so that no consumer thread adds more than 2^15 rows (which keeps
 // its 32-bit and 64-bit partial sums exact) and per-launch sums stay below 2^31 rows.
 uint64_t scan_max_rows_per_launch(int layout, int placement, uint32_t grid);
 

@@ -163,6 +163,72 @@ struct Quad {
     uint32_t a[4];    // 100 - discount
     uint32_t ab[4];   // (100 - discount) * (100 + tax)
     uint32_t p[4];    // extendedprice
+    uint32_t A;       // bytes r: 100 - discount
+    uint32_t P[4];    // byte planes of the prices: byte r of P[k] = byte k of p[r]
+    uint32_t ABL, ABH;  // bytes r: low / high byte of ab[r]
+};
+
+// Byte planes of four 32-bit words (a 4x4 byte transpose, eight byte permutes).
+__device__ __forceinline__ void byte_planes(const uint32_t w[4], uint32_t out[4]) {
+    const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140u), t1 = __byte_perm(w[2], w[3], 0x5140u);
+    const uint32_t t2 = __byte_perm(w[0], w[1], 0x7362u), t3 = __byte_perm(w[2], w[3], 0x7362u);
+    out[0] = __byte_perm(t0, t1, 0x5410u);
+    out[1] = __byte_perm(t0, t1, 0x7632u);
+    out[2] = __byte_perm(t2, t3, 0x5410u);
+    out[3] = __byte_perm(t2, t3, 0x7632u);
+}
+
+// Aggregates of one group, per thread, computed with byte dot products (dp4a: four rows per
+// instruction). With W1 = 0/1 bytes of the group's rows and M = its 0x00/0xFF byte mask:
+//   count, qty, disc      dp4a(W1, 1 | Q | D)
+//   sum p                 sum_k 2^8k dp4a(W1, P_k)
+//   sum (100-d) p         sum_k 2^8k dp4a(A & M, P_k)
+//   sum (100-d)(100+t) p  sum_k 2^8k (dp4a(ABL & M, P_k) + 2^8 dp4a(ABH & M, P_k))
+// Every 32-bit partial stays exact while a thread adds at most 2^15 rows per launch (the host
+// caps launches accordingly): the largest, an ab-low plane, grows by <= 4*255*255 per quad.
+struct GroupPlanes {
+    uint32_t cnt, q, d;
+    uint32_t p[4], dp[4], chl[4], chh[4];
+    __device__ __forceinline__ void zero() {
+        cnt = q = d = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) p[k] = dp[k] = chl[k] = chh[k] = 0;
+    }
+    __device__ __forceinline__ void add_quad(uint32_t OH, uint32_t g, const Quad& x) {
+        const uint32_t W1 = (OH >> g) & 0x01010101u;
+        const uint32_t M = (W1 << 8) - W1;   // 0xFF in the group's row bytes
+        const uint32_t MA = x.A & M, ML = x.ABL & M, MH = x.ABH & M;
+        cnt = __dp4a(W1, 0x01010101u, cnt);
+        q = __dp4a(W1, x.Q, q);
+        d = __dp4a(W1, x.D, d);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            p[k] = __dp4a(W1, x.P[k], p[k]);
+            dp[k] = __dp4a(MA, x.P[k], dp[k]);
+            chl[k] = __dp4a(ML, x.P[k], chl[k]);
+            chh[k] = __dp4a(MH, x.P[k], chh[k]);
+        }
+    }
+    __device__ __forceinline__ uint64_t value(int agg) const {
+        uint64_t v = 0;
+        switch (agg) {
+            case kAggCount: return cnt;
+            case kAggQty: return q;
+            case kAggDisc: return d;
+            case kAggBasePrice:
+#pragma unroll
+                for (int k = 0; k < 4; ++k) v += (uint64_t)p[k] << (8 * k);
+                return v;
+            case kAggDiscPrice:
+#pragma unroll
+                for (int k = 0; k < 4; ++k) v += (uint64_t)dp[k] << (8 * k);
+                return v;
+            default:
+#pragma unroll
+                for (int k = 0; k < 4; ++k) v += ((uint64_t)chl[k] << (8 * k)) + ((uint64_t)chh[k] << (8 * k + 8));
+                return v;
+        }
+    }
 };
 
 // Code of row r of a quad (0..7 = group code, 7 also = filtered out) for row-wise placements.
@@ -174,8 +240,8 @@ __device__ __forceinline__ uint32_t quad_code(const Quad& x, int r) {
 // Aggregates of one group, per thread, fed a quad at a time. W1 (byte r = 1 iff row r is in the
 // group) drives three byte dot products (count, quantity, discount of 4 rows in one dp4a each);
 // the price products use the FMA pipe: pg = m * p (m in {0,1}), then wide multiply-adds.
-// 32-bit count/quantity/discount partials stay exact: a thread adds at most 2^16 rows per launch
-// (the host caps rows per launch at 2^16 per consumer thread), so quantity <= 255 * 2^16.
+// 32-bit count/quantity/discount partials stay exact: a thread adds at most 2^15 rows per launch
+// (the host caps rows per launch at 2^15 per consumer thread), so quantity <= 255 * 2^15.
 struct GroupQuadRegs {
     uint64_t p, dp, ch;
     uint32_t cnt, q, d;
@@ -222,7 +288,7 @@ struct CtaRed {
 template <int G, bool kWideQty>
 struct AccPerThread {
     GroupRegs<kWideQty> g[kWideQty ? G : 1];      // row-wise path (uncompressed layout)
-    GroupQuadRegs gq[kWideQty ? 1 : G];           // quad path (compressed layouts)
+    GroupPlanes gq[kWideQty ? 1 : G];             // quad path (compressed layouts)
     __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
 #pragma unroll
         for (int i = 0; i < (kWideQty ? G : 1); ++i) g[i].zero();
@@ -239,17 +305,20 @@ struct AccPerThread {
             x.OH = c < (uint32_t)G ? (1u << c) : 0u;
             x.Q = q;
             x.D = d;
-            x.a[0] = a;
-            x.ab[0] = ab;
-            x.p[0] = p;
-            x.a[1] = x.a[2] = x.a[3] = x.ab[1] = x.ab[2] = x.ab[3] = x.p[1] = x.p[2] = x.p[3] = 0;
+            x.A = a;
+            x.P[0] = p & 0xFFu;
+            x.P[1] = (p >> 8) & 0xFFu;
+            x.P[2] = (p >> 16) & 0xFFu;
+            x.P[3] = p >> 24;
+            x.ABL = ab & 0xFFu;
+            x.ABH = ab >> 8;
             add_quad(x);
         }
     }
     __device__ __forceinline__ void add_quad(const Quad& x) {
         if constexpr (!kWideQty) {
 #pragma unroll
-            for (int i = 0; i < G; ++i) gq[i].add_quad((x.OH >> i) & 0x01010101u, x);
+            for (int i = 0; i < G; ++i) gq[i].add_quad(x.OH, (uint32_t)i, x);
         }
     }
     __device__ __forceinline__ void fold() {
@@ -534,6 +603,7 @@ __device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t 
         }
         x.OH = OH & PM;
         const uint32_t A = 0x64646464u - x.D;   // 100 - d per byte (no borrow inside the domain)
+        x.A = A;
         x.p[0] = P.x;
         x.p[1] = P.y;
         x.p[2] = P.z;
@@ -542,6 +612,12 @@ __device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t 
         for (int r = 0; r < 4; ++r) {
             x.a[r] = __byte_perm(A, 0u, 0x4440u | (uint32_t)r);
             x.ab[r] = x.a[r] * (100u + __byte_perm(X, 0u, 0x4440u | (uint32_t)r));
+        }
+        byte_planes(x.p, x.P);
+        {
+            const uint32_t u = __byte_perm(x.ab[0], x.ab[1], 0x5140u), v = __byte_perm(x.ab[2], x.ab[3], 0x5140u);
+            x.ABL = __byte_perm(u, v, 0x5410u);
+            x.ABH = __byte_perm(u, v, 0x7632u);
         }
         acc.add_quad(x);
     }
@@ -807,7 +883,7 @@ uint64_t scan_max_rows_per_launch(int layout, int placement, uint32_t grid) {
     // accumulating lanes per CTA: every consumer thread, or the lanes of one warp-lane table
     const uint64_t codes = (layout == kLayPair || layout == kLayPairFilter) ? 4 : 6;
     const uint64_t lanes = placement == kPlaceInRegisters ? kConsumerWarps * (32 / codes) : kConsumerWarps * 32;
-    uint64_t n = (uint64_t)grid * lanes * 65536ull;
+    uint64_t n = (uint64_t)grid * lanes * 32768ull;
     if (n > (1ull << 31)) n = 1ull << 31;
     const uint64_t tile = scan_tile_rows(layout);
     return n / tile * tile;
