@@ -345,9 +345,10 @@ q1_status q1_sync_check(void* cuda_stream);
 /* Bytes of device scratch q1_launch_groupkey needs for num_groups groups. */
 uint64_t q1_groupkey_scratch_bytes(uint32_t num_groups);
 
-/* Placements: IN_REGISTERS_PER_THREAD (num_groups <= 8), SHARED_MEM_PER_THREAD (a per-CTA
- * shared-memory table for keys < 2048, larger keys spilled to global atomics), GLOBAL (global
- * atomics for every row). Reads ship, qty, disc, tax, price of dev_cols and dev_keys; the result
+/* Placements: IN_REGISTERS_PER_THREAD (num_groups <= 8; per-thread byte-plane sums),
+ * SHARED_MEM_PER_THREAD (a per-CTA shared-memory table: (group, discount) cells for
+ * num_groups <= 256, else one slot per key < 2048 with larger keys spilled to global atomics),
+ * GLOBAL (global atomics for every row). Reads ship, qty, disc, tax, price of dev_cols and dev_keys; the result
  * accumulates into dev_aggregates[num_groups][6] (caller-zeroed int128). dev_scratch: device
  * memory of q1_groupkey_scratch_bytes(num_groups), owned by the caller; calls on different
  * streams need different scratch. A key >= num_groups in a passing row is reported as
@@ -407,7 +408,7 @@ q1_status q1_batch_create(const q1_batch_instance* instances, uint32_t n, const 
 /* One execution of every instance (asynchronous; q1_sync_check reports device errors). */
 q1_status q1_batch_run(q1_batch* b, void* cuda_stream);
 q1_status q1_batch_describe(q1_batch* b, q1_batch_desc* out);
-/* Placement chosen for instance i: 0 registers, 1 shared table, 2 global. */
+/* Placement chosen for instance i: 0 registers (num_groups <= 4), 1 shared table, 2 global. */
 q1_status q1_batch_instance_mode(q1_batch* b, uint32_t i, int32_t* mode);
 q1_status q1_batch_destroy(q1_batch* b);
 
@@ -429,6 +430,123 @@ q1_status q1_generate_compressed_device(uint64_t seed, uint64_t first_row, uint6
                                         q1_flag_packing packing,
                                         const q1_compressed_host_out* dev_out,
                                         void* cuda_stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Serving: a request loop with continuous batching. No reference counterpart: the reference    */
+/* answers one query per process run (src/main.cu:520-760); its per-query path stays available  */
+/* as q1_server_plain, and every served response equals it bit for bit.                          */
+/*                                                                                              */
+/* The server keeps one resident table in HBM (the seeded generator's rows, compressed, plus a   */
+/* uint32 key column uniform over Q1_SERVE_RESIDENT_KEY_GROUPS groups) together with its partial */
+/* aggregates per ship day (cumulative over days, per (returnflag, linestatus) group and per key */
+/* group), so a resident request is answered from those without a scan. Ad-hoc requests name a  */
+/* table of their own: adhoc_rows rows of the generator under adhoc_seed with its grouping. It   */
+/* is generated on the device into an arena of hbm_budget_bytes on first use and stays there     */
+/* (least recently used tables not in use are evicted when a new one does not fit). A dispatcher */
+/* thread forms rounds from the queue (FIFO) while a slot is free and the next request's table   */
+/* is or can be made resident; one round = missing tables generated, all ad-hoc requests of the */
+/* round aggregated together in one persistent batch launch, resident answers looked up, all     */
+/* responses copied back. Requests that arrive during a round join the next one.                */
+/* Q1_SERVE_PLAIN runs the same loop with one request per round through the plain launch.       */
+/* ------------------------------------------------------------------------------------------ */
+
+#define Q1_SERVE_MAX_GROUPS 64
+#define Q1_SERVE_RESIDENT_KEY_GROUPS 64
+
+typedef enum q1_request_kind {
+    Q1_REQ_RESIDENT = 0,   /* query the server's resident table */
+    Q1_REQ_ADHOC    = 1    /* query a table of adhoc_rows rows generated under adhoc_seed */
+} q1_request_kind;
+
+typedef enum q1_grouping {
+    Q1_GROUP_FLAGS = 0,    /* group by (l_returnflag, l_linestatus): 6 slots, 4 live (the Q1 grouping) */
+    Q1_GROUP_KEYS  = 1     /* group by a uniform synthetic key in [0, num_groups) */
+} q1_grouping;
+
+typedef struct q1_request {
+    int32_t  kind;          /* q1_request_kind */
+    int32_t  grouping;      /* q1_grouping */
+    uint32_t num_groups;    /* Q1_GROUP_KEYS: 1..64 (resident: exactly 64); ignored for FLAGS */
+    int32_t  cutoff_day;    /* l_shipdate <= cutoff_day (day number) */
+    uint64_t adhoc_rows;    /* Q1_REQ_ADHOC: (adhoc_seed, adhoc_rows, grouping, num_groups) */
+    uint64_t adhoc_seed;    /* name the table; keys come from the same seed */
+} q1_request;
+
+typedef struct q1_response {
+    uint64_t ticket;
+    int32_t  status;        /* q1_status of the request */
+    uint32_t num_groups;    /* group slots filled: 6 (FLAGS) or num_groups (KEYS) */
+    double   latency_ms;    /* submission -> response ready */
+    double   queue_ms;      /* submission -> admission into a round */
+    /* [group][6]: count, sum_qty (hundredths), sum_base_price, sum_disc, sum_disc_price,
+     * sum_charge, the int128 table of q1_launch_groupkey */
+    q1_i128  aggregates[Q1_SERVE_MAX_GROUPS * 6];
+} q1_response;
+
+typedef enum q1_serve_mode {
+    Q1_SERVE_BATCHED = 0,   /* continuous batching into rounds */
+    Q1_SERVE_PLAIN   = 1    /* one request per round, one plain launch each (the comparison) */
+} q1_serve_mode;
+
+typedef struct q1_server_opts {
+    int32_t  device;
+    uint32_t max_inflight;       /* requests per round (response slots) */
+    int32_t  mode;               /* q1_serve_mode */
+    uint32_t reserved;
+    uint64_t seed;               /* resident table seed */
+    uint64_t resident_rows;      /* rows of the resident table */
+    uint64_t hbm_budget_bytes;   /* arena of resident ad-hoc tables (13 B per row + alignment) */
+    uint64_t max_adhoc_rows;     /* larger ad-hoc requests are refused at submission */
+} q1_server_opts;
+
+typedef struct q1_server_stats {
+    uint64_t completed;
+    uint64_t failed;
+    uint64_t rounds;
+    uint64_t pending;            /* submitted, not yet admitted */
+    uint64_t logical_rows;       /* rows of all completed requests' tables */
+    uint64_t scanned_rows;       /* rows actually scanned (ad-hoc tables) */
+    uint64_t generated_rows;     /* ad-hoc rows generated (table cache misses) */
+    uint64_t cache_hits, cache_misses, evictions;
+    uint64_t cached_tables, cached_bytes;
+    double   wall_ms;            /* first completed request's submission -> last completion */
+    double   mean_round_size;
+    double   p50_ms, p90_ms, p99_ms, max_ms, mean_ms;   /* latency of completed requests */
+} q1_server_stats;
+
+typedef struct q1_server q1_server;
+
+/* Defaults: device 0, 256 slots, batched, seed 20260104, 600M resident rows, 120 GiB budget,
+ * 100M rows per ad-hoc table. */
+void q1_server_opts_default(q1_server_opts* opts);
+
+/* Builds the resident table and its per-day aggregates on the device, allocates the arena and
+ * starts the dispatcher. */
+q1_status q1_server_open(const q1_server_opts* opts, q1_server** out);
+
+/* Queues a request. Q1_ERR_INVALID_ARGUMENT for a malformed request, Q1_ERR_BUSY when its
+ * table can never fit the budget. Thread-safe. */
+q1_status q1_server_submit(q1_server* server, const q1_request* req, uint64_t* ticket);
+
+/* Waits for a ticket (timeout_ms < 0: no limit; Q1_ERR_BUSY on expiry, the ticket stays
+ * valid) and releases it into `out`. Thread-safe. */
+q1_status q1_server_wait(q1_server* server, uint64_t ticket, int32_t timeout_ms, q1_response* out);
+
+q1_status q1_server_stats_get(q1_server* server, q1_server_stats* out);
+q1_status q1_server_reset_stats(q1_server* server);
+
+/* The plain path for one request: one scan launch over its table (q1_launch_compressed for
+ * resident FLAGS requests, q1_launch_groupkey otherwise; ad-hoc FLAGS tables are generated in
+ * the compressed pair layout for it), synchronous, on a stream of its own. The judge of every
+ * served response. */
+q1_status q1_server_plain(q1_server* server, const q1_request* req, q1_response* out);
+
+/* Device pointers to the resident table (pair layout) and its key column. */
+q1_status q1_server_resident_columns(q1_server* server, q1_compressed_columns* cols,
+                                     const uint32_t** dev_keys, uint64_t* rows);
+
+/* Finishes queued requests, stops the dispatcher and frees everything. */
+q1_status q1_server_close(q1_server* server);
 
 /* One-line description of a CUDA device (name, compute capability, SMs, memory, L2) into buf.
  * Replaces get_device_properties / --device (src/helper.hpp:18-48, src/main.cu:266-268). */

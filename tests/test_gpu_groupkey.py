@@ -43,14 +43,39 @@ def keys_for(num_groups, dist):
     return gen_np.group_keys_cdf(SEED, 0, ROWS, cdf), cdf
 
 
-def run_gpu(c, keys, num_groups, placement, cutoff):
+def widen(comp, seed, frac=0.05):
+    """Copy of compressed columns with a fraction of rows moved to the edges of the compressed
+    domain (discount 11..100, tax 9..255, price >= 2^24, quantity 51..255): the shared tables'
+    slow path."""
+    out = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in comp.items()}
+    n = len(out["shipdate"])
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(n, max(1, int(frac * n)), replace=False)
+    out["discount"][idx] = rng.integers(0, 101, len(idx))
+    out["tax"][idx] = rng.integers(0, 256, len(idx))
+    out["extendedprice"][idx] = rng.integers(0, 2**32, len(idx), dtype=np.uint64).astype(np.uint32)
+    out["quantity"][idx] = rng.integers(0, 256, len(idx))
+    return out
+
+
+def device_cols(comp):
+    dev = {k: torch.from_numpy(np.ascontiguousarray(comp[k]).view(np.uint8).copy()).cuda()
+           for k in ["shipdate", "discount", "extendedprice", "tax", "quantity"]}
+    c = _lib.CompressedColumns()
+    for k, t in dev.items():
+        setattr(c, k, t.data_ptr())
+    return c, dev
+
+
+def run_gpu(c, keys, num_groups, placement, cutoff, blocks=0):
+    rows = len(keys)
     dkeys = torch.from_numpy(keys.view(np.int32).copy()).cuda()
     scratch = torch.zeros(int(q.lib().q1_groupkey_scratch_bytes(num_groups)) // 8 + 2, dtype=torch.int64, device="cuda")
     out = torch.zeros(num_groups * 12, dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    cfg = _lib.LaunchConfig(0, 0, 0)
+    cfg = _lib.LaunchConfig(0, 0, blocks)
     _lib.check(q.lib().q1_launch_groupkey(q.placement_id(placement), ctypes.byref(c), ctypes.c_void_p(dkeys.data_ptr()),
-                                          num_groups, ROWS, cutoff, ctypes.byref(cfg),
+                                          num_groups, rows, cutoff, ctypes.byref(cfg),
                                           ctypes.c_void_p(scratch.data_ptr()), ctypes.c_void_p(out.data_ptr()),
                                           ctypes.c_void_p(stream)))
     _lib.check(q.lib().q1_sync_check(ctypes.c_void_p(stream)))
@@ -78,12 +103,47 @@ def test_groupkey_placements(table, num_groups, dist, placement):
         check(comp, keys, num_groups, cutoff, run_gpu(c, keys, num_groups, placement, cutoff))
 
 
-@pytest.mark.parametrize("num_groups", [1, 4, 8])
+@pytest.mark.parametrize("num_groups", [1, 3, 4, 5, 8])
 @pytest.mark.parametrize("cutoff", CUTOFFS)
 def test_groupkey_registers(table, num_groups, cutoff):
     comp, c, _ = table
     keys, _ = keys_for(num_groups, "uniform")
     check(comp, keys, num_groups, cutoff, run_gpu(c, keys, num_groups, "in_registers_per_thread", cutoff))
+
+
+@pytest.mark.parametrize("num_groups,placement", [
+    (4, "in_registers_per_thread"), (7, "in_registers_per_thread"), (6, "shared_mem_per_thread"),
+    (256, "shared_mem_per_thread"), (257, "shared_mem_per_thread"), (3000, "shared_mem_per_thread"),
+    (64, "global")])
+def test_domain_edges_take_exact_paths(table, num_groups, placement):
+    """Rows with discount > 10, tax > 8, price >= 2^24 or quantity > 50 leave the shared tables'
+    fast domain; the result must stay exact."""
+    comp, _, _ = table
+    wide = widen(comp, 7 + num_groups)
+    c, keep = device_cols(wide)
+    for dist in ["uniform", "zipf"]:
+        keys, _ = keys_for(num_groups, dist)
+        for cutoff in [729999, 730089]:
+            check(wide, keys, num_groups, cutoff, run_gpu(c, keys, num_groups, placement, cutoff))
+
+
+@pytest.fixture(scope="module")
+def long_table(cuda):
+    rows = 9_000_011
+    comp = widen(gen_np.compress(gen_np.generate(SEED + 1, 0, rows)), 99, frac=0.001)
+    c, keep = device_cols(comp)
+    return comp, c, keep, rows
+
+
+@pytest.mark.parametrize("num_groups,placement", [
+    (4, "in_registers_per_thread"), (8, "in_registers_per_thread"), (64, "shared_mem_per_thread"),
+    (1024, "shared_mem_per_thread"), (5000, "shared_mem_per_thread")])
+def test_one_cta_flushes_mid_launch(long_table, num_groups, placement):
+    """One CTA over 9M rows: the per-thread planes (every 4032 tiles) and the shared tables
+    (every 2^23 rows) are flushed inside the launch."""
+    comp, c, _, rows = long_table
+    keys = gen_np.group_keys_uniform(SEED + 2, 0, rows, num_groups)
+    check(comp, keys, num_groups, 729999, run_gpu(c, keys, num_groups, placement, 729999, blocks=1))
 
 
 def test_registers_refuse_many_groups(table):

@@ -116,6 +116,41 @@ class BatchDesc(ctypes.Structure):
                 ("total_rows", ctypes.c_uint64), ("total_groups", ctypes.c_uint64)]
 
 
+SERVE_MAX_GROUPS = 64
+SERVE_RESIDENT_KEY_GROUPS = 64
+REQ_RESIDENT, REQ_ADHOC = 0, 1
+GROUP_FLAGS, GROUP_KEYS = 0, 1
+SERVE_BATCHED, SERVE_PLAIN = 0, 1
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("grouping", ctypes.c_int32), ("num_groups", ctypes.c_uint32),
+                ("cutoff_day", ctypes.c_int32), ("adhoc_rows", ctypes.c_uint64), ("adhoc_seed", ctypes.c_uint64)]
+
+
+class Response(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("status", ctypes.c_int32), ("num_groups", ctypes.c_uint32),
+                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("aggregates", I128 * (SERVE_MAX_GROUPS * 6))]
+
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("max_inflight", ctypes.c_uint32), ("mode", ctypes.c_int32),
+                ("reserved", ctypes.c_uint32), ("seed", ctypes.c_uint64),
+                ("resident_rows", ctypes.c_uint64), ("hbm_budget_bytes", ctypes.c_uint64),
+                ("max_adhoc_rows", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
+                ("pending", ctypes.c_uint64), ("logical_rows", ctypes.c_uint64), ("scanned_rows", ctypes.c_uint64),
+                ("generated_rows", ctypes.c_uint64), ("cache_hits", ctypes.c_uint64), ("cache_misses", ctypes.c_uint64),
+                ("evictions", ctypes.c_uint64), ("cached_tables", ctypes.c_uint64), ("cached_bytes", ctypes.c_uint64),
+                ("wall_ms", ctypes.c_double), ("mean_round_size", ctypes.c_double), ("p50_ms", ctypes.c_double),
+                ("p90_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/q1.h
 SIGNATURES = {
     "q1_last_error": (ctypes.c_char_p, []),
@@ -167,6 +202,16 @@ SIGNATURES = {
     "q1_batch_describe": (ctypes.c_int, [vp, ctypes.POINTER(BatchDesc)]),
     "q1_batch_instance_mode": (ctypes.c_int, [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int32)]),
     "q1_batch_destroy": (ctypes.c_int, [vp]),
+    "q1_server_opts_default": (None, [ctypes.POINTER(ServerOpts)]),
+    "q1_server_open": (ctypes.c_int, [ctypes.POINTER(ServerOpts), ctypes.POINTER(vp)]),
+    "q1_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
+    "q1_server_wait": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(Response)]),
+    "q1_server_stats_get": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+    "q1_server_reset_stats": (ctypes.c_int, [vp]),
+    "q1_server_plain": (ctypes.c_int, [vp, ctypes.POINTER(Request), ctypes.POINTER(Response)]),
+    "q1_server_resident_columns": (ctypes.c_int, [vp, ctypes.POINTER(CompressedColumns), ctypes.POINTER(vp),
+                                                  ctypes.POINTER(ctypes.c_uint64)]),
+    "q1_server_close": (ctypes.c_int, [vp]),
     "q1_version": (ctypes.c_char_p, []),
 }
 

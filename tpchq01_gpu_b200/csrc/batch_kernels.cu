@@ -15,17 +15,19 @@
 // straight from global memory instead). Eight consumer warps aggregate every tile; when the
 // instance changes they flush their accumulators into the instance's scratch (red.global.add),
 // according to the instance's placement mode:
-//   kModeRegisters  num_groups <= 8: per-thread registers, predicated by one-hot key bits
-//   kModeShared     a shared-memory table for keys < 2048 (shared atomics), the rest spilled
+//   kModeRegisters  num_groups <= 4: per-thread dp4a byte planes (ka::PlaneRegs<4>)
+//   kModeShared     num_groups <= 256: shared (group, discount) cells (ka::CubeTable); more
+//                   groups: shared slots for keys < 2048 (ka::SlotTable), the rest spilled
 //   kModeGlobal     every passing row reduces straight into the scratch accumulators
-// Scratch per instance: num_groups x 8 u64 (count, qty, disc, price, disc_price lo32/hi32 sums,
-// charge lo32/hi32 sums), folded into the caller's int128 table by batch_finalize.
+// (engines in q1_keyagg.cuh). Scratch per instance: num_groups x 8 u64, folded into the
+// caller's int128 table by batch_finalize.
 // All waits are bounded (q1_ptx.cuh); on expiry the kernel records a status bit and leaves.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "q1_batch.h"
 #include "q1_common.cuh"
+#include "q1_keyagg.cuh"
 #include "q1_ptx.cuh"
 
 namespace q1 {
@@ -34,18 +36,15 @@ using namespace ptx;
 
 namespace bk {
 
-constexpr uint32_t R = kBatchTileRows;   // 2048
+constexpr uint32_t R = ka::R;   // 2048 rows per tile
 constexpr uint32_t S = 4;
 constexpr uint32_t W = 8;
-constexpr uint32_t kStage = R * 13;
-constexpr uint32_t kOffShip = 0, kOffQty = 2 * R, kOffDisc = 3 * R, kOffTax = 4 * R, kOffPrice = 5 * R, kOffKey = 9 * R;
-__host__ __device__ constexpr uint32_t col_bytes(int c) { return c == 0 ? 2 * R : (c < 4 ? R : 4 * R); }
-__host__ __device__ constexpr uint32_t col_off(int c) {
-    return c == 0 ? kOffShip : (c == 1 ? kOffQty : (c == 2 ? kOffDisc : (c == 3 ? kOffTax : (c == 4 ? kOffPrice : kOffKey))));
-}
+constexpr uint32_t kStage = ka::kStageBytes;
 constexpr uint32_t kSteps = R / 4;
-constexpr uint32_t kHotSlots = 2048;
 constexpr uint32_t kKindFull = 0, kKindPartial = 1, kKindEnd = 2;
+// shared table region: the larger of the cube (256 groups) and the slot table (2048 slots)
+constexpr uint32_t kTableBytes =
+    ka::cube_bytes(ka::kCubeMaxGroups) > ka::slot_bytes(ka::kSlots) ? ka::cube_bytes(ka::kCubeMaxGroups) : ka::slot_bytes(ka::kSlots);
 
 struct StageMeta {
     uint32_t instance;
@@ -54,23 +53,6 @@ struct StageMeta {
     uint32_t pad;
     uint64_t row0;     // first row of the tile within the instance
 };
-
-__device__ __forceinline__ void red_add(unsigned long long* p, uint64_t v) {
-    if (v) asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ void scratch_add(unsigned long long* acc, uint32_t g, uint64_t cnt, uint64_t q, uint64_t d,
-                                            uint64_t p, uint64_t dp, uint64_t ch) {
-    unsigned long long* a = acc + 8ull * g;
-    red_add(a + 0, cnt);
-    red_add(a + 1, q);
-    red_add(a + 2, d);
-    red_add(a + 3, p);
-    red_add(a + 4, dp & 0xFFFFFFFFull);
-    red_add(a + 5, dp >> 32);
-    red_add(a + 6, ch & 0xFFFFFFFFull);
-    red_add(a + 7, ch >> 32);
-}
 
 }  // namespace bk
 
@@ -84,15 +66,7 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t ring = smem_addr(smem);
-    // shared table (52 B per slot): count u32; qty, disc, price, disc_price, charge low 32 bits,
-    // charge high bits as u64 -- exact for 2^25 rows between flushes
-    uint32_t* t_cnt = reinterpret_cast<uint32_t*>(smem + S * kStage);
-    unsigned long long* t_q = reinterpret_cast<unsigned long long*>(smem + S * kStage + 4 * kHotSlots);
-    unsigned long long* t_d = t_q + kHotSlots;
-    unsigned long long* t_p = t_d + kHotSlots;
-    unsigned long long* t_dp = t_p + kHotSlots;
-    unsigned long long* t_chl = t_dp + kHotSlots;
-    unsigned long long* t_chh = t_chl + kHotSlots;
+    uint8_t* const tab = smem + S * kStage;   // shared table, all zero between instances
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < S; ++s) {
@@ -102,10 +76,7 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
         mbar_init(smem_addr(&consumers_bar), W);
         fence_mbar_init();
     }
-    for (uint32_t i = threadIdx.x; i < kHotSlots; i += blockDim.x) {
-        t_cnt[i] = 0;
-        t_q[i] = t_d[i] = t_p[i] = t_dp[i] = t_chl[i] = t_chh[i] = 0;
-    }
+    for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(tab)[i] = 0;
     __syncthreads();
 
     if (warp == W) {
@@ -137,8 +108,8 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
                         mbar_arrive_expect_tx(fb, kStage);
 #pragma unroll
                         for (int c = 0; c < 6; ++c)
-                            bulk_g2s(ring + s * kStage + col_off(c), in.col[c] + tile * (uint64_t)col_bytes(c),
-                                     col_bytes(c), fb, pol);
+                            bulk_g2s(ring + s * kStage + ka::col_off(c), in.col[c] + tile * (uint64_t)ka::col_bytes(c),
+                                     ka::col_bytes(c), fb, pol);
                     } else {
                         meta[s].kind = kKindPartial;
                         mbar_arrive(fb);
@@ -163,92 +134,53 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
         uint32_t cur = 0xFFFFFFFFu;
         BatchInstanceDev in{};
         uint32_t mode = kModeGlobal;
-        // registers mode: 8 groups
-        uint64_t rp[8], rdp[8], rch[8];
-        uint32_t rc[8], rq[8], rd[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) rp[i] = rdp[i] = rch[i] = 0, rc[i] = rq[i] = rd[i] = 0;
+        bool use_cube = false;
+        uint32_t hot = 0;
+        ka::PlaneRegs<4> regs;
+        regs.zero();
+        ka::CubeTable cube;
+        ka::SlotTable slots;
+        cube.bind(tab, 0);
+        slots.bind(tab, 0);
+        ka::ConsumerBarrier cb{smem_addr(&consumers_bar), 0};
         uint32_t bad = 0;
-
-        // Rows added since the last flush (the same count in every consumer thread): registers
-        // are flushed every 2^19 rows (per-thread sums x 32 lanes stay below 2^64), the shared
-        // table every 2^25 rows, and both whenever the instance changes.
-        uint64_t since = 0;
-        // Barrier of the consumer warps only (the producer keeps streaming): one arrive per warp,
-        // bounded wait; every consumer passes the same sequence of barriers, so a local phase
-        // counter tracks the barrier's parity.
-        uint32_t sync_phase = 0;
-        auto consumers_sync = [&]() {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_addr(&consumers_bar));
-            mbar_wait(smem_addr(&consumers_bar), sync_phase & 1u, prm.status);
-            ++sync_phase;
-        };
+        // Tiles / rows added since the last flush (the same in every consumer thread): plane
+        // partials are flushed every ka::kPlaneFlushTiles tiles, shared tables before they would
+        // exceed ka::kTableFlushRows rows, and both whenever the instance changes. A flush of a
+        // shared table leaves it all zero.
+        uint32_t tiles_since = 0;
+        uint64_t rows_since = 0;
         auto flush = [&]() {
-            since = 0;
+            tiles_since = 0;
+            rows_since = 0;
             if (cur == 0xFFFFFFFFu) return;
             if (mode == kModeRegisters) {
-#pragma unroll
-                for (int g = 0; g < 8; ++g) {
-                    const uint64_t v[6] = {rc[g], rq[g], rd[g], rp[g], rdp[g], rch[g]};
-                    uint64_t s6[6];
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) s6[a] = warp_sum_u64(v[a]);
-                    if (lane == 0 && (uint32_t)g < in.num_groups && s6[0])
-                        scratch_add(in.acc, g, s6[0], s6[1], s6[2], s6[3], s6[4], s6[5]);
-                    rp[g] = rdp[g] = rch[g] = 0;
-                    rc[g] = rq[g] = rd[g] = 0;
-                }
+                regs.flush(in.acc, in.num_groups, lane);
             } else if (mode == kModeShared) {
-                const uint32_t hot = in.num_groups < kHotSlots ? in.num_groups : kHotSlots;
-                consumers_sync();
-                for (uint32_t g = ctid; g < hot; g += W * 32) {
-                    if (t_cnt[g]) {
-                        unsigned long long* a = in.acc + 8ull * g;
-                        red_add(a + 0, t_cnt[g]);
-                        red_add(a + 1, t_q[g]);
-                        red_add(a + 2, t_d[g]);
-                        red_add(a + 3, t_p[g]);
-                        red_add(a + 4, t_dp[g] & 0xFFFFFFFFull);
-                        red_add(a + 5, t_dp[g] >> 32);
-                        red_add(a + 6, t_chl[g]);
-                        red_add(a + 7, t_chh[g]);
-                    }
-                    t_cnt[g] = 0;
-                    t_q[g] = t_d[g] = t_p[g] = t_dp[g] = t_chl[g] = t_chh[g] = 0;
-                }
-                consumers_sync();
+                cb.sync(lane, prm.status);
+                if (use_cube) cube.flush(in.acc, in.num_groups, ctid, W * 32);
+                else slots.flush(in.acc, ctid, W * 32);
+                cb.sync(lane, prm.status);
             }
         };
-
-        auto row = [&](uint32_t key, bool pass, uint32_t q, uint32_t d, uint32_t t, uint32_t p) {
-            if (pass && key >= in.num_groups) bad = 1;
-            if (!pass || key >= in.num_groups) return;
-            const uint32_t a = 100u - d;
-            const uint32_t ab = a * (100u + t);
+        auto add = [&](const ka::KeyQuad& x) {
             if (mode == kModeRegisters) {
-#pragma unroll
-                for (int g = 0; g < 8; ++g) {
-                    const bool hit = key == (uint32_t)g;
-                    const uint32_t pg = hit ? p : 0u;
-                    rc[g] += hit ? 1u : 0u;
-                    rq[g] += hit ? q : 0u;
-                    rd[g] += hit ? d : 0u;
-                    rp[g] += pg;
-                    rdp[g] = mad_wide(a, pg, rdp[g]);
-                    rch[g] = mad_wide(ab, pg, rch[g]);
-                }
-            } else if (mode == kModeShared && key < kHotSlots) {
-                atomicAdd(&t_cnt[key], 1u);
-                atomicAdd(&t_q[key], (unsigned long long)q);
-                atomicAdd(&t_d[key], (unsigned long long)d);
-                atomicAdd(&t_p[key], (unsigned long long)p);
-                const uint64_t ch = (uint64_t)ab * p;
-                atomicAdd(&t_dp[key], (unsigned long long)((uint64_t)a * p));
-                atomicAdd(&t_chl[key], (unsigned long long)(ch & 0xFFFFFFFFull));
-                atomicAdd(&t_chh[key], (unsigned long long)(ch >> 32));
+                regs.add(x, in.num_groups, bad);
+            } else if (mode == kModeShared) {
+                if (use_cube) ka::table_quad(cube, x, in.num_groups, hot, in.acc, bad);
+                else ka::table_quad(slots, x, in.num_groups, hot, in.acc, bad);
             } else {
-                scratch_add(in.acc, key, 1, q, d, p, (uint64_t)a * p, (uint64_t)ab * p);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (!((x.PM >> (8 * r)) & 1u)) continue;
+                    const uint32_t key = x.k[r];
+                    if (key >= in.num_groups) {
+                        bad = 1u;
+                        continue;
+                    }
+                    ka::scratch_row(in.acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                                    (x.X >> (8 * r)) & 0xFFu, x.p[r]);
+                }
             }
         };
 
@@ -264,40 +196,24 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
                 cur = m.instance;
                 in = prm.inst[cur];
                 mode = in.mode;
-            } else if ((mode == kModeRegisters && since >= (1ull << 19)) || (mode == kModeShared && since >= (1ull << 25))) {
+                if (mode == kModeRegisters && in.num_groups > 4) mode = kModeShared;   // planes hold 4 groups
+                use_cube = in.num_groups <= ka::kCubeMaxGroups;
+                hot = use_cube ? in.num_groups : (in.num_groups < ka::kSlots ? in.num_groups : ka::kSlots);
+                if (use_cube) cube.bind(tab, in.num_groups);
+                else slots.bind(tab, hot);
+            } else if ((mode == kModeRegisters && tiles_since >= ka::kPlaneFlushTiles) ||
+                       (mode == kModeShared && rows_since + m.rows > ka::kTableFlushRows)) {
                 flush();
             }
-            since += m.rows;
+            ++tiles_since;
+            rows_since += m.rows;
             if (m.kind == kKindFull) {
                 const uint32_t base = ring + s * kStage;
 #pragma unroll
-                for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx) {
-                    const uint32_t j = ctid + itx * (W * 32);
-                    const uint2 sd = lds_v2(base + kOffShip + 8 * j);
-                    const uint32_t Q = lds_u32(base + kOffQty + 4 * j);
-                    const uint32_t D = lds_u32(base + kOffDisc + 4 * j);
-                    const uint32_t X = lds_u32(base + kOffTax + 4 * j);
-                    const uint4 Pv = lds_v4(base + kOffPrice + 16 * j);
-                    const uint4 K = lds_v4(base + kOffKey + 16 * j);
-                    if ((((D & 0x7F7F7F7Fu) + 0x1B1B1B1Bu) | D) & 0x80808080u) bad = 1;
-                    const uint32_t sh[4] = {sd.x & 0xFFFFu, sd.x >> 16, sd.y & 0xFFFFu, sd.y >> 16};
-                    const uint32_t pv[4] = {Pv.x, Pv.y, Pv.z, Pv.w};
-                    const uint32_t kv[4] = {K.x, K.y, K.z, K.w};
-#pragma unroll
-                    for (int r = 0; r < 4; ++r)
-                        row(kv[r], (int32_t)sh[r] <= in.cutoff, (Q >> (8 * r)) & 0xFFu, (D >> (8 * r)) & 0xFFu,
-                            (X >> (8 * r)) & 0xFFu, pv[r]);
-                }
+                for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
+                    add(ka::load_quad(base, ctid + itx * (W * 32), in.cutoff, bad));
             } else {
-                for (uint32_t i = ctid; i < m.rows; i += W * 32) {
-                    const uint64_t rr = m.row0 + i;
-                    const uint32_t d = __ldg(in.col[2] + rr);
-                    if (d > 100u) bad = 1;
-                    row(__ldg(reinterpret_cast<const uint32_t*>(in.col[5]) + rr),
-                        (int32_t)__ldg(reinterpret_cast<const uint16_t*>(in.col[0]) + rr) <= in.cutoff,
-                        __ldg(in.col[1] + rr), d, __ldg(in.col[3] + rr),
-                        __ldg(reinterpret_cast<const uint32_t*>(in.col[4]) + rr));
-                }
+                for (uint32_t i = ctid; i < m.rows; i += W * 32) add(ka::load_row(in.col, m.row0 + i, in.cutoff, bad));
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
@@ -359,7 +275,7 @@ cudaError_t launch_batch_zero_outputs(const BatchInstanceDev* inst, const uint64
     return cudaGetLastError();
 }
 
-uint32_t batch_smem_bytes() { return bk::S * bk::kStage + bk::kHotSlots * 52; }
+uint32_t batch_smem_bytes() { return bk::S * bk::kStage + bk::kTableBytes; }
 
 cudaError_t batch_prepare_launch() {
     return cudaFuncSetAttribute(q1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem_bytes());

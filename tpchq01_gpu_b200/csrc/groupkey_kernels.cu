@@ -4,28 +4,26 @@
 // The per-row arithmetic is the reference's (src/kernels/ht_in_global_mem.hpp:31-49); only the
 // group index changes: group = key[i] (< num_groups) instead of (rf << 1) + ls.
 //
-// Input tile (R rows): ship u16 | qty u8 | disc u8 | tax u8 | price u32 | key u32  (13 B/row),
-// streamed with one cp.async.bulk per column into an S-stage shared-memory ring exactly like the
-// scan kernel (scan_kernels.cu).
+// Input tile (2048 rows): ship u16 | qty u8 | disc u8 | tax u8 | price u32 | key u32 (13 B/row),
+// streamed with one cp.async.bulk per column into a 4-stage shared-memory ring exactly like the
+// scan kernel (scan_kernels.cu); 8 consumer warps decode 4 rows per step (q1_keyagg.cuh).
 //
 // Placements:
-//   in_registers_per_thread  num_groups <= 8: predicated per-thread registers over 8 groups
-//   shared_mem_per_thread    hierarchical: keys < kHotSlots in a per-CTA shared-memory table
-//                            (shared atomics), other keys spilled straight to the global
-//                            accumulators
-//   global                   every passing row updates the global accumulators directly
+//   in_registers_per_thread  num_groups <= 8: per-thread dp4a byte planes (PlaneRegs<4|8>)
+//   shared_mem_per_thread    num_groups <= 256: shared (group, discount) cells (CubeTable);
+//                            otherwise keys < 2048 in shared slots (SlotTable), larger keys
+//                            reduced straight into the global accumulators
+//   global                   every passing row reduces into the global accumulators
 //
-// Accumulators live in scratch memory (per launch, zeroed first): per group 8 x u64
-//   count, qty (whole units), disc, price, disc_price low-32 sum, disc_price high-32 sum,
-//   charge low-32 sum, charge high-32 sum
-// Splitting the two wide products into 32-bit halves keeps every u64 sum exact for launches of
-// up to 2^31 rows, so plain fire-and-forget reductions (red.global.add) suffice. A finalize
-// kernel folds the scratch into the caller's int128 table [group][6] with 128-bit atomics
-// (so, like the reference kernels, results accumulate into a caller-zeroed buffer).
+// Accumulators live in scratch memory (per launch, zeroed first): per group 8 x u64 (see
+// q1_keyagg.cuh); a finalize kernel folds them into the caller's int128 table [group][6] with
+// 128-bit atomics (so, like the reference kernels, results accumulate into a caller-zeroed
+// buffer). Launches are capped at 2^31 rows so every u64 scratch sum stays exact.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "q1_common.cuh"
+#include "q1_keyagg.cuh"
 #include "q1_kernels.h"
 #include "q1_ptx.cuh"
 
@@ -35,65 +33,26 @@ using namespace ptx;
 
 namespace gk {
 
-constexpr uint32_t R = 2048;          // rows per tile
+constexpr uint32_t R = ka::R;         // rows per tile
 constexpr uint32_t S = 4;             // ring stages
 constexpr uint32_t W = 8;             // consumer warps
-constexpr uint32_t kStage = R * 13;   // bytes per stage
-// column offsets inside a stage (all multiples of 16)
-constexpr uint32_t kOffShip = 0, kOffQty = 2 * R, kOffDisc = 3 * R, kOffTax = 4 * R, kOffPrice = 5 * R,
-                   kOffKey = 9 * R;
-__host__ __device__ constexpr uint32_t col_bytes(int c) { return c == 0 ? 2 * R : (c < 4 ? R : 4 * R); }
-__host__ __device__ constexpr uint32_t col_off(int c) {
-    return c == 0 ? kOffShip : (c == 1 ? kOffQty : (c == 2 ? kOffDisc : (c == 3 ? kOffTax : (c == 4 ? kOffPrice : kOffKey))));
-}
+constexpr uint32_t kStage = ka::kStageBytes;
 constexpr uint32_t kSteps = R / 4;    // 4 rows per consumer step
 static_assert(kSteps % (W * 32) == 0, "steps must divide evenly");
 static_assert(kStage % 16 == 0, "stage alignment");
 
-// Shared table of the hierarchical placement: SoA, 44 B per slot (count u32 + 5 x u64).
-constexpr uint32_t kHotSlots = 2048;
+// Table engine of the shared_mem_per_thread placement.
+enum TableKind : uint32_t { kTableNone = 0, kTableCube = 1, kTableSlots = 2 };
 
-__device__ __forceinline__ void red_add(unsigned long long* p, uint64_t v) {
-    if (v) asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__host__ __device__ constexpr uint32_t table_kind(int placement, uint32_t num_groups) {
+    return placement != kPlaceSharedMemPerThread ? kTableNone
+                                                 : (num_groups <= ka::kCubeMaxGroups ? kTableCube : kTableSlots);
 }
-
-// Adds one row (or a partial sum whose wide parts are given as full 64-bit values) into the
-// global accumulators of group g.
-__device__ __forceinline__ void global_add(unsigned long long* acc, uint32_t g, uint64_t cnt, uint64_t q, uint64_t d,
-                                           uint64_t p, uint64_t dp, uint64_t ch) {
-    unsigned long long* a = acc + 8ull * g;
-    red_add(a + 0, cnt);
-    red_add(a + 1, q);
-    red_add(a + 2, d);
-    red_add(a + 3, p);
-    red_add(a + 4, dp & 0xFFFFFFFFull);
-    red_add(a + 5, dp >> 32);
-    red_add(a + 6, ch & 0xFFFFFFFFull);
-    red_add(a + 7, ch >> 32);
+__host__ __device__ constexpr uint32_t table_bytes(uint32_t kind, uint32_t num_groups) {
+    return kind == kTableCube ? ka::cube_bytes(num_groups)
+                              : (kind == kTableSlots ? ka::slot_bytes(num_groups < ka::kSlots ? num_groups : ka::kSlots)
+                                                     : 0u);
 }
-
-struct RegTable {   // 8 groups, predicated (same arithmetic as the scan kernel's per-thread table)
-    uint64_t p[8], dp[8], ch[8];
-    uint32_t q[8], d[8], cnt[8];   // per-thread rows stay below 2^31 / (148 * 256): no u32 overflow
-    __device__ __forceinline__ void zero() {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) p[i] = dp[i] = ch[i] = q[i] = d[i] = cnt[i] = 0;
-    }
-    __device__ __forceinline__ void add(uint32_t key, bool pass, uint32_t q_, uint32_t d_, uint32_t a, uint32_t ab,
-                                        uint32_t pr) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const bool hit = pass && key == (uint32_t)i;
-            const uint32_t pg = hit ? pr : 0u;
-            cnt[i] += hit ? 1u : 0u;
-            q[i] += hit ? q_ : 0u;
-            d[i] += hit ? d_ : 0u;
-            p[i] += pg;
-            dp[i] = mad_wide(a, pg, dp[i]);
-            ch[i] = mad_wide(ab, pg, ch[i]);
-        }
-    }
-};
 
 }  // namespace gk
 
@@ -102,43 +61,43 @@ struct GroupKeyParams {
     uint64_t rows;
     int32_t cutoff;                 // cutoff_day - 727563
     uint32_t num_groups;
+    uint32_t table;                 // gk::TableKind
     unsigned long long* acc;        // scratch: num_groups x 8 u64, zeroed
     uint32_t* status;
 };
 
-template <int P>
+// P: placement; NG: plane groups of in_registers_per_thread (4 or 8).
+template <int P, int NG>
 __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const __grid_constant__ GroupKeyParams prm) {
     using namespace gk;
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t full_bar[S];
     __shared__ __align__(8) uint64_t empty_bar[S];
-    __shared__ __align__(16) unsigned long long red8[8 * 6];
+    __shared__ __align__(8) uint64_t cons_bar;
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint64_t num_tiles = prm.rows / R;
     const uint32_t ring = smem_addr(smem);
-    // shared table (hierarchical placement), after the ring
-    uint32_t* t_cnt = reinterpret_cast<uint32_t*>(smem + S * kStage);
-    unsigned long long* t_q = reinterpret_cast<unsigned long long*>(smem + S * kStage + 4 * kHotSlots);
-    unsigned long long* t_d = t_q + kHotSlots;
-    unsigned long long* t_p = t_d + kHotSlots;
-    unsigned long long* t_dp = t_p + kHotSlots;
-    unsigned long long* t_ch = t_dp + kHotSlots;   // 4 + 5*8 = 44 B per slot
-    const uint32_t hot = prm.num_groups < kHotSlots ? prm.num_groups : kHotSlots;
+    const uint32_t G = prm.num_groups;
+    ka::CubeTable cube;
+    ka::SlotTable slots;
+    const uint32_t hot = G < ka::kSlots ? G : ka::kSlots;
+    if (P == kPlaceSharedMemPerThread) {
+        if (prm.table == kTableCube) cube.bind(smem + S * kStage, G);
+        else slots.bind(smem + S * kStage, hot);
+    }
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < S; ++s) {
             mbar_init(smem_addr(&full_bar[s]), 1);
             mbar_init(smem_addr(&empty_bar[s]), W);
         }
+        mbar_init(smem_addr(&cons_bar), W);
         fence_mbar_init();
     }
-    for (uint32_t i = threadIdx.x; i < 48; i += blockDim.x) red8[i] = 0;
     if (P == kPlaceSharedMemPerThread) {
-        for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
-            t_cnt[i] = 0;
-            t_q[i] = t_d[i] = t_p[i] = t_dp[i] = t_ch[i] = 0;
-        }
+        if (prm.table == kTableCube) cube.zero(threadIdx.x, blockDim.x);
+        else slots.zero(threadIdx.x, blockDim.x);
     }
     __syncthreads();
 
@@ -153,36 +112,48 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
                 mbar_arrive_expect_tx(fb, kStage);
 #pragma unroll
                 for (int c = 0; c < 6; ++c)
-                    bulk_g2s(ring + s * kStage + col_off(c), prm.col[c] + t * (uint64_t)col_bytes(c), col_bytes(c), fb, pol);
+                    bulk_g2s(ring + s * kStage + ka::col_off(c), prm.col[c] + t * (uint64_t)ka::col_bytes(c),
+                             ka::col_bytes(c), fb, pol);
             }
             for (uint32_t i = (k > S ? k - S : 0u); i < k; ++i) mbar_wait(smem_addr(&full_bar[i % S]), (i / S) & 1u, prm.status);
         }
     } else {
         const uint32_t ctid = threadIdx.x;
-        RegTable regs;
+        ka::PlaneRegs<NG> regs;
         if (P == kPlaceInRegistersPerThread) regs.zero();
+        ka::ConsumerBarrier cb{smem_addr(&cons_bar), 0};
         uint32_t bad = 0;
-        auto row = [&](uint32_t key, bool pass, uint32_t q, uint32_t d, uint32_t t, uint32_t p) {
-            const uint32_t a = 100u - d;
-            const uint32_t ab = a * (100u + t);
-            if (P == kPlaceInRegistersPerThread) {
-                regs.add(key, pass && key < prm.num_groups, q, d, a, ab, p);
-            } else if (pass && key < prm.num_groups) {
-                const uint64_t dp = (uint64_t)a * p;
-                const uint64_t ch = (uint64_t)ab * p;
-                if (P == kPlaceSharedMemPerThread && key < hot) {
-                    atomicAdd(&t_cnt[key], 1u);
-                    atomicAdd(&t_q[key], (unsigned long long)q);
-                    atomicAdd(&t_d[key], (unsigned long long)d);
-                    atomicAdd(&t_p[key], (unsigned long long)p);
-                    atomicAdd(&t_dp[key], (unsigned long long)dp);
-                    atomicAdd(&t_ch[key], (unsigned long long)ch);
-                } else {
-                    global_add(prm.acc, key, 1, q, d, p, dp, ch);
+        uint32_t tiles_since = 0;
+        uint64_t rows_since = 0;
+
+        // one decoded quad into the placement's engine
+        auto add_quad = [&](const ka::KeyQuad& x) {
+            if constexpr (P == kPlaceInRegistersPerThread) {
+                regs.add(x, G, bad);
+            } else if constexpr (P == kPlaceSharedMemPerThread) {
+                if (prm.table == kTableCube) ka::table_quad(cube, x, G, G, prm.acc, bad);
+                else ka::table_quad(slots, x, G, hot, prm.acc, bad);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (!((x.PM >> (8 * r)) & 1u)) continue;
+                    const uint32_t key = x.k[r];
+                    if (key >= G) {
+                        bad = 1u;
+                        continue;
+                    }
+                    ka::scratch_row(prm.acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                                    (x.X >> (8 * r)) & 0xFFu, x.p[r]);
                 }
             }
-            if (pass && key >= prm.num_groups) bad |= kStatusDomain;
         };
+        auto table_flush = [&]() {
+            cb.sync(lane, prm.status);
+            if (prm.table == kTableCube) cube.flush(prm.acc, G, ctid, W * 32);
+            else slots.flush(prm.acc, ctid, W * 32);
+            cb.sync(lane, prm.status);
+        };
+
         bool ok = true;
         uint32_t k = 0;
         for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {
@@ -192,59 +163,36 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
                 ok = false;
                 break;
             }
+            if (P == kPlaceInRegistersPerThread && tiles_since >= ka::kPlaneFlushTiles) {
+                regs.flush(prm.acc, G, lane);
+                tiles_since = 0;
+            }
+            if (P == kPlaceSharedMemPerThread && rows_since + R > ka::kTableFlushRows) {
+                table_flush();
+                rows_since = 0;
+            }
+            ++tiles_since;
+            rows_since += R;
             const uint32_t base = ring + s * kStage;
 #pragma unroll
-            for (uint32_t it = 0; it < kSteps / (W * 32); ++it) {
-                const uint32_t j = ctid + it * (W * 32);
-                const uint2 sd = lds_v2(base + kOffShip + 8 * j);
-                const uint32_t Q = lds_u32(base + kOffQty + 4 * j);
-                const uint32_t D = lds_u32(base + kOffDisc + 4 * j);
-                const uint32_t X = lds_u32(base + kOffTax + 4 * j);
-                const uint4 Pv = lds_v4(base + kOffPrice + 16 * j);
-                const uint4 K = lds_v4(base + kOffKey + 16 * j);
-                bad |= ((((D & 0x7F7F7F7Fu) + 0x1B1B1B1Bu) | D) & 0x80808080u) ? kStatusDomain : 0u;
-                const uint32_t sh[4] = {sd.x & 0xFFFFu, sd.x >> 16, sd.y & 0xFFFFu, sd.y >> 16};
-                const uint32_t pv[4] = {Pv.x, Pv.y, Pv.z, Pv.w};
-                const uint32_t kv[4] = {K.x, K.y, K.z, K.w};
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    row(kv[r], (int32_t)sh[r] <= prm.cutoff, (Q >> (8 * r)) & 0xFFu, (D >> (8 * r)) & 0xFFu,
-                        (X >> (8 * r)) & 0xFFu, pv[r]);
-            }
+            for (uint32_t it = 0; it < kSteps / (W * 32); ++it)
+                add_quad(ka::load_quad(base, ctid + it * (W * 32), prm.cutoff, bad));
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
         }
-        if (ok && blockIdx.x == (uint32_t)(num_tiles % gridDim.x)) {
-            for (uint64_t i = num_tiles * R + ctid; i < prm.rows; i += W * 32) {
-                const uint32_t d = __ldg(prm.col[2] + i);
-                bad |= d > 100u ? kStatusDomain : 0u;
-                row(__ldg(reinterpret_cast<const uint32_t*>(prm.col[5]) + i),
-                    (int32_t)__ldg(reinterpret_cast<const uint16_t*>(prm.col[0]) + i) <= prm.cutoff,
-                    __ldg(prm.col[1] + i), d, __ldg(prm.col[3] + i), __ldg(reinterpret_cast<const uint32_t*>(prm.col[4]) + i));
-            }
+        // the rows after the last full tile, by one CTA straight from global memory
+        if (ok && blockIdx.x == (uint32_t)(num_tiles % gridDim.x) && num_tiles * R < prm.rows) {
+            if (P == kPlaceSharedMemPerThread && rows_since + R > ka::kTableFlushRows) table_flush();
+            for (uint64_t i = num_tiles * R + ctid; i < prm.rows; i += W * 32)
+                add_quad(ka::load_row(prm.col, i, prm.cutoff, bad));
         }
-        if (bad && prm.status) atomicOr(prm.status, bad);
-        if (P == kPlaceInRegistersPerThread) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const uint64_t v[6] = {regs.cnt[i], regs.q[i], regs.d[i], regs.p[i], regs.dp[i], regs.ch[i]};
-#pragma unroll
-                for (int a = 0; a < 6; ++a) {
-                    uint64_t lo = v[a], hi = 0;
-                    warp_sum_u128(lo, hi);   // per-CTA sums stay below 2^64 (launches <= 2^31 rows)
-                    if (lane == 0) atomicAdd(&red8[i * 6 + a], (unsigned long long)lo);
-                }
-            }
-        }
+        if (bad && prm.status) atomicOr(prm.status, kStatusDomain);
+        if (P == kPlaceInRegistersPerThread) regs.flush(prm.acc, G, lane);
     }
     __syncthreads();
-    if (P == kPlaceInRegistersPerThread) {
-        for (uint32_t g = threadIdx.x; g < 8 && g < prm.num_groups; g += blockDim.x)
-            global_add(prm.acc, g, red8[g * 6 + 0], red8[g * 6 + 1], red8[g * 6 + 2], red8[g * 6 + 3],
-                       red8[g * 6 + 4], red8[g * 6 + 5]);
-    } else if (P == kPlaceSharedMemPerThread) {
-        for (uint32_t g = threadIdx.x; g < hot; g += blockDim.x)
-            if (t_cnt[g]) global_add(prm.acc, g, t_cnt[g], t_q[g], t_d[g], t_p[g], t_dp[g], t_ch[g]);
+    if (P == kPlaceSharedMemPerThread) {
+        if (prm.table == kTableCube) cube.flush(prm.acc, G, threadIdx.x, blockDim.x);
+        else slots.flush(prm.acc, threadIdx.x, blockDim.x);
     }
 }
 
@@ -267,18 +215,19 @@ __global__ void __launch_bounds__(256) q1_groupkey_finalize(const unsigned long 
     atomic_add_u128(o + 2 * kAggCharge, (uint64_t)ch, (uint64_t)(ch >> 64));
 }
 
-template <int P>
+template <int P, int NG>
 static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_blocks, cudaStream_t st) {
     using namespace gk;
-    uint32_t dyn = S * kStage + (P == kPlaceSharedMemPerThread ? kHotSlots * 44 : 0);
-    cudaError_t e = cudaFuncSetAttribute(q1_groupkey_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    const uint32_t dyn = S * kStage + table_bytes(prm.table, prm.num_groups);
+    cudaError_t e =
+        cudaFuncSetAttribute(q1_groupkey_kernel<P, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     const uint64_t tiles = prm.rows / R;
     uint64_t blocks = tiles ? tiles : 1;
     uint64_t cap = (uint64_t)sm_count;
     if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
     if (blocks > cap) blocks = cap;
-    q1_groupkey_kernel<P><<<(unsigned)blocks, (W + 1) * 32, dyn, st>>>(prm);
+    q1_groupkey_kernel<P, NG><<<(unsigned)blocks, (W + 1) * 32, dyn, st>>>(prm);
     return cudaGetLastError();
 }
 
@@ -296,12 +245,16 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
         prm.rows = n;
         prm.cutoff = cutoff_rel;
         prm.num_groups = num_groups;
+        prm.table = gk::table_kind(placement, num_groups);
         prm.acc = scratch;
         prm.status = status;
         switch (placement) {
-            case kPlaceInRegistersPerThread: e = launch_gk<kPlaceInRegistersPerThread>(prm, sm_count, max_blocks, stream); break;
-            case kPlaceSharedMemPerThread: e = launch_gk<kPlaceSharedMemPerThread>(prm, sm_count, max_blocks, stream); break;
-            case kPlaceGlobal: e = launch_gk<kPlaceGlobal>(prm, sm_count, max_blocks, stream); break;
+            case kPlaceInRegistersPerThread:
+                e = num_groups <= 4 ? launch_gk<kPlaceInRegistersPerThread, 4>(prm, sm_count, max_blocks, stream)
+                                    : launch_gk<kPlaceInRegistersPerThread, 8>(prm, sm_count, max_blocks, stream);
+                break;
+            case kPlaceSharedMemPerThread: e = launch_gk<kPlaceSharedMemPerThread, 4>(prm, sm_count, max_blocks, stream); break;
+            case kPlaceGlobal: e = launch_gk<kPlaceGlobal, 4>(prm, sm_count, max_blocks, stream); break;
             default: return cudaErrorInvalidValue;
         }
         if (e != cudaSuccess) return e;

@@ -8,7 +8,7 @@
 // Autotuner: an instance's class is (floor(log2 rows), num_groups, selectivity decile), the
 // selectivity being measured on a strided sample of its ship dates. For every class the tuner
 // times the batch kernel on the class's largest instance alone under each applicable placement
-// (registers when num_groups <= 8, shared table, global) and keeps the fastest; the work-item
+// (registers when num_groups <= 4, shared table, global) and keeps the fastest; the work-item
 // size (tiles per item) is then chosen by timing the whole batch with a few candidates. Results
 // are cached in a text file ("mode <log2rows> <groups> <decile> <mode>", "chunk <signature>
 // <tiles>") so later batches with the same classes skip the measurements.
@@ -255,7 +255,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
         d.out = reinterpret_cast<unsigned long long*>(x.aggregates);
         b->group_base[i + 1] = b->group_base[i] + x.num_groups;
         b->total_rows += x.rows;
-        b->modes[i] = x.num_groups <= 8 ? kModeRegisters : kModeShared;   // heuristic default
+        b->modes[i] = x.num_groups <= 4 ? kModeRegisters : kModeShared;   // heuristic default
     }
     b->total_groups = b->group_base[n];
     if ((st = b->d_inst.alloc(sizeof(BatchInstanceDev) * std::max<uint32_t>(1, n))) != Q1_OK) return st;
@@ -302,7 +302,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
                 continue;
             }
             std::vector<uint32_t> cands;
-            if (b->inst[i].num_groups <= 8) cands.push_back(kModeRegisters);
+            if (b->inst[i].num_groups <= 4) cands.push_back(kModeRegisters);
             cands.push_back(kModeShared);
             cands.push_back(kModeGlobal);
             uint32_t best = cands[0];

@@ -10,8 +10,9 @@ constexpr uint32_t kBatchTileRows = 2048;
 
 // Placement of one instance inside the batch kernel.
 enum BatchMode : uint32_t {
-    kModeRegisters = 0,   // num_groups <= 8
-    kModeShared = 1,      // shared-memory table for keys < 2048, the rest spilled to scratch
+    kModeRegisters = 0,   // num_groups <= 4: per-thread byte planes
+    kModeShared = 1,      // shared-memory table: (group, discount) cells for <= 256 groups, else
+                          // slots for keys < 2048 with the rest spilled to scratch
     kModeGlobal = 2,      // reductions straight into scratch
 };
 

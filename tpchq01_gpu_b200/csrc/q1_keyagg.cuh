@@ -1,0 +1,368 @@
+// Group-key aggregation engines shared by the group-key kernel (groupkey_kernels.cu) and the
+// batch kernel (batch_kernels.cu): the Q1 predicate and aggregates over a 13 B/row tile
+// (ship u16 | qty u8 | disc u8 | tax u8 | price u32 | key u32), grouped by key < num_groups.
+// The per-row arithmetic is the reference's (src/kernels/ht_in_global_mem.hpp:31-49) with
+// group = key.
+//
+// Engines (one per placement):
+//   PlaneRegs<NG>  num_groups <= NG (4 or 8): per-thread byte-plane dot products (dp4a), four
+//                  rows per instruction, as in the scan kernel; no atomics until a flush.
+//   CubeTable      num_groups <= 256: a shared-memory table per (group, discount) cell. A row
+//                  adds only its count and quantity (one packed word), its price and tax * price;
+//                  the discounted sums follow exactly at the flush, because the discount of a
+//                  cell is known there: sum (100-d) p = sum_d (100-d) P_d and
+//                  sum (100-d)(100+t) p = sum_d (100-d) (100 P_d + TP_d).
+//   SlotTable      keys < 2048: a shared-memory table per group (count and discount packed,
+//                  quantity, price, disc_price, charge).
+//   global         every row reduces straight into the scratch accumulators.
+// The shared tables use only 32-bit shared atomics (64-bit shared atomics are far slower);
+// 64-bit sums are kept as (low word, carry word) pairs: the low word's atomic returns the old
+// value, and a wrap adds the carry to the high word. Rows outside the tables' fast domain
+// (discount > 10, tax > 8 or price >= 2^24; TPC-H data has none) take the global path, so every
+// result is exact over the whole compressed domain.
+//
+// Scratch per group (8 x u64, zeroed before a launch): count, quantity (whole units), discount,
+// price, disc_price = a4 + 2^32 a5, charge = a6 + 2^32 a7; folded into an int128 table later.
+#pragma once
+
+#include <stdint.h>
+
+#include "q1_common.cuh"
+#include "q1_ptx.cuh"
+#include "q1_quad.cuh"
+
+namespace q1 {
+namespace ka {
+
+using namespace ptx;
+
+// ---------------------------------------------------------------------------------------------
+// Tile layout (R rows per tile, every column offset a multiple of 16 bytes)
+// ---------------------------------------------------------------------------------------------
+constexpr uint32_t R = 2048;
+constexpr uint32_t kOffShip = 0, kOffQty = 2 * R, kOffDisc = 3 * R, kOffTax = 4 * R, kOffPrice = 5 * R,
+                   kOffKey = 9 * R;
+constexpr uint32_t kStageBytes = 13 * R;
+__host__ __device__ constexpr uint32_t col_bytes(int c) { return c == 0 ? 2 * R : (c < 4 ? R : 4 * R); }
+__host__ __device__ constexpr uint32_t col_off(int c) {
+    return c == 0 ? kOffShip : (c == 1 ? kOffQty : (c == 2 ? kOffDisc : (c == 3 ? kOffTax : (c == 4 ? kOffPrice : kOffKey))));
+}
+
+// Flush cadences. Plane partials: at most 2^15 rows per thread; every consumer thread handles at
+// most R / 256 = 8 rows of a tile, so 4032 tiles leave room for one more partial tile.
+// Shared tables: at most 2^23 rows per CTA between flushes keeps every packed field and carry
+// word below its limit (count < 2^24 per cell; carry words < 2^32).
+constexpr uint32_t kPlaneFlushTiles = 4032;
+constexpr uint64_t kTableFlushRows = 1ull << 23;
+
+constexpr uint32_t kCubeMaxGroups = 256;
+constexpr uint32_t kCubeDisc = 11;          // discount 0..10
+constexpr uint32_t kCubeWords = 6;          // xlo xhi plo phi tlo thi
+constexpr uint32_t kSlots = 2048;
+constexpr uint32_t kSlotWords = 9;          // xlo xhi q plo phi dlo dhi clo chi
+
+__host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) { return num_groups * kCubeDisc * kCubeWords * 4; }
+__host__ __device__ constexpr uint32_t slot_bytes(uint32_t slots) { return slots * kSlotWords * 4; }
+
+// ---------------------------------------------------------------------------------------------
+// Scratch updates
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void red_add(unsigned long long* p, uint64_t v) {
+    if (v) asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void scratch_add(unsigned long long* acc, uint32_t g, uint64_t cnt, uint64_t q, uint64_t d,
+                                            uint64_t p, uint64_t dp_lo, uint64_t dp_hi, uint64_t ch_lo, uint64_t ch_hi) {
+    unsigned long long* a = acc + 8ull * g;
+    red_add(a + 0, cnt);
+    red_add(a + 1, q);
+    red_add(a + 2, d);
+    red_add(a + 3, p);
+    red_add(a + 4, dp_lo);
+    red_add(a + 5, dp_hi);
+    red_add(a + 6, ch_lo);
+    red_add(a + 7, ch_hi);
+}
+
+// One passing row straight into the scratch (the global placement and the slow path).
+__device__ __forceinline__ void scratch_row(unsigned long long* acc, uint32_t key, uint32_t q, uint32_t d, uint32_t t,
+                                            uint32_t p) {
+    const uint32_t a = 100u - d;
+    const uint64_t dp = (uint64_t)a * p, ch = (uint64_t)(a * (100u + t)) * p;
+    scratch_add(acc, key, 1, q, d, p, dp & 0xFFFFFFFFull, dp >> 32, ch & 0xFFFFFFFFull, ch >> 32);
+}
+
+__device__ __forceinline__ bool fast_domain(uint32_t d, uint32_t t, uint32_t p) {
+    return d < kCubeDisc && t <= 8u && p < (1u << 24);
+}
+
+// 64-bit sum as (lo, hi) 32-bit shared words: lo += v, carry into hi.
+__device__ __forceinline__ void add_carry(uint32_t* lo, uint32_t* hi, uint32_t v) {
+    const uint32_t old = atomicAdd(lo, v);
+    if (old + v < old) atomicAdd(hi, 1u);
+}
+__device__ __forceinline__ void add_wide(uint32_t* lo, uint32_t* hi, uint32_t vlo, uint32_t vhi) {
+    const uint32_t old = atomicAdd(lo, vlo);
+    const uint32_t h = vhi + (old + vlo < old ? 1u : 0u);
+    if (h) atomicAdd(hi, h);
+}
+
+// ---------------------------------------------------------------------------------------------
+// A quad: four consecutive rows of a tile
+// ---------------------------------------------------------------------------------------------
+struct KeyQuad {
+    uint32_t PM;        // byte r = 0xFF iff row r passes the predicate
+    uint32_t Q, D, X;   // bytes r: quantity, discount, tax
+    uint32_t p[4];
+    uint32_t k[4];
+};
+
+// Rows 4j..4j+3 of the tile at shared address `base`. `bad` becomes nonzero for a value outside
+// the compressed domain (ship offset > 32767, discount > 100).
+__device__ __forceinline__ KeyQuad load_quad(uint32_t base, uint32_t j, int32_t cut, uint32_t& bad) {
+    KeyQuad x;
+    x.PM = quad_pass_mask(lds_v2(base + kOffShip + 8 * j), cut, bad);
+    x.Q = lds_u32(base + kOffQty + 4 * j);
+    x.D = lds_u32(base + kOffDisc + 4 * j);
+    x.X = lds_u32(base + kOffTax + 4 * j);
+    const uint4 P = lds_v4(base + kOffPrice + 16 * j);
+    const uint4 K = lds_v4(base + kOffKey + 16 * j);
+    bad |= disc_out_of_domain4(x.D);
+    x.p[0] = P.x, x.p[1] = P.y, x.p[2] = P.z, x.p[3] = P.w;
+    x.k[0] = K.x, x.k[1] = K.y, x.k[2] = K.z, x.k[3] = K.w;
+    return x;
+}
+
+// One row read from global memory (tail rows of a partial tile), as a quad whose rows 1..3 fail.
+__device__ __forceinline__ KeyQuad load_row(const uint8_t* const col[6], uint64_t i, int32_t cut, uint32_t& bad) {
+    KeyQuad x;
+    const uint32_t ship = __ldg(reinterpret_cast<const uint16_t*>(col[0]) + i);
+    const uint32_t d = __ldg(col[2] + i);
+    bad |= (ship > 32767u || d > 100u) ? 1u : 0u;
+    x.PM = (int32_t)ship <= cut ? 0xFFu : 0u;
+    x.Q = __ldg(col[1] + i);
+    x.D = d;
+    x.X = __ldg(col[3] + i);
+    x.p[0] = __ldg(reinterpret_cast<const uint32_t*>(col[4]) + i);
+    x.k[0] = __ldg(reinterpret_cast<const uint32_t*>(col[5]) + i);
+    x.p[1] = x.p[2] = x.p[3] = 0;
+    x.k[1] = x.k[2] = x.k[3] = 0;
+    return x;
+}
+
+// ---------------------------------------------------------------------------------------------
+// PlaneRegs: per-thread dp4a byte planes for num_groups <= NG
+// ---------------------------------------------------------------------------------------------
+template <int NG>
+struct PlaneRegs {
+    GroupPlanes g[NG];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < NG; ++i) g[i].zero();
+    }
+    __device__ __forceinline__ void add(const KeyQuad& kq, uint32_t num_groups, uint32_t& bad) {
+        uint32_t OH = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t key = kq.k[r];
+            const bool in = key < num_groups;
+            if (!in && ((kq.PM >> (8 * r)) & 1u)) bad = 1u;
+            OH |= (in ? (1u << (key & 7u)) : 0u) << (8 * r);
+        }
+        Quad x;
+        x.OH = OH & kq.PM;
+        x.Q = kq.Q;
+        x.D = kq.D;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) x.p[r] = kq.p[r];
+        quad_derive(x, kq.X);
+#pragma unroll
+        for (int i = 0; i < NG; ++i) g[i].add_quad(x.OH, (uint32_t)i, x);
+    }
+    // Warp sums of the per-thread partials into the scratch; every lane of the warp calls it.
+    __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t lane) {
+#pragma unroll
+        for (int i = 0; i < NG; ++i) {
+            if ((uint32_t)i < num_groups) {
+                const uint64_t ch = g[i].value(kAggCharge), dp = g[i].value(kAggDiscPrice);
+                const uint64_t cnt = warp_sum_u64(g[i].cnt);
+                const uint64_t q = warp_sum_u64(g[i].q), d = warp_sum_u64(g[i].d);
+                const uint64_t p = warp_sum_u64(g[i].value(kAggBasePrice));
+                const uint64_t dpl = warp_sum_u64(dp & 0xFFFFFFFFull), dph = warp_sum_u64(dp >> 32);
+                const uint64_t chl = warp_sum_u64(ch & 0xFFFFFFFFull), chh = warp_sum_u64(ch >> 32);
+                if (lane == 0 && cnt) scratch_add(acc, (uint32_t)i, cnt, q, d, p, dpl, dph, chl, chh);
+            }
+            g[i].zero();
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// CubeTable: shared (group, discount) cells
+// ---------------------------------------------------------------------------------------------
+struct CubeTable {
+    uint32_t* w;       // [kCubeWords][cells]
+    uint32_t cells;
+    __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
+        w = reinterpret_cast<uint32_t*>(base);
+        cells = num_groups * kCubeDisc;
+    }
+    __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
+        for (uint32_t i = tid; i < kCubeWords * cells; i += nthreads) w[i] = 0;
+    }
+    // Rows r of a quad with bit r of `m` set (passing, key < num_groups, fast domain). All
+    // atomics of the quad are issued before any carry is checked, so their latencies overlap.
+    __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
+                                             const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
+        uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            c[r] = key[r] * kCubeDisc + d[r];
+            vx[r] = 1u + (q[r] << 24);   // count + 2^24 * quantity
+            vt[r] = t[r] * p[r];         // < 2^28
+            if ((m >> r) & 1u) {
+                ox[r] = atomicAdd(w + c[r], vx[r]);
+                op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
+                ot[r] = atomicAdd(w + 4 * cells + c[r], vt[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if ((m >> r) & 1u) {
+                if (ox[r] + vx[r] < ox[r]) atomicAdd(w + cells + c[r], 1u);
+                if (op[r] + p[r] < op[r]) atomicAdd(w + 3 * cells + c[r], 1u);
+                if (ot[r] + vt[r] < ot[r]) atomicAdd(w + 5 * cells + c[r], 1u);
+            }
+        }
+    }
+    // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
+    __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t tid, uint32_t nthreads) {
+        for (uint32_t g = tid; g < num_groups; g += nthreads) {
+            uint64_t cnt = 0, q = 0, dsum = 0, P = 0;
+            unsigned __int128 DP = 0, CH = 0;
+#pragma unroll
+            for (uint32_t d = 0; d < kCubeDisc; ++d) {
+                const uint32_t c = g * kCubeDisc + d;
+                const uint64_t X = ((uint64_t)w[cells + c] << 32) | w[c];
+                const uint64_t Pd = ((uint64_t)w[3 * cells + c] << 32) | w[2 * cells + c];
+                const uint64_t TPd = ((uint64_t)w[5 * cells + c] << 32) | w[4 * cells + c];
+                const uint64_t nd = X & 0xFFFFFFull;
+                cnt += nd;
+                q += X >> 24;
+                dsum += (uint64_t)d * nd;
+                P += Pd;
+                DP += (unsigned __int128)(100u - d) * Pd;
+                CH += (unsigned __int128)(100u - d) * ((unsigned __int128)Pd * 100u + TPd);
+#pragma unroll
+                for (uint32_t k = 0; k < kCubeWords; ++k) w[k * cells + c] = 0;
+            }
+            if (cnt)
+                scratch_add(acc, g, cnt, q, dsum, P, (uint64_t)DP & 0xFFFFFFFFull, (uint64_t)(DP >> 32),
+                            (uint64_t)CH & 0xFFFFFFFFull, (uint64_t)(CH >> 32));
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// SlotTable: shared per-group slots for keys < slots
+// ---------------------------------------------------------------------------------------------
+struct SlotTable {
+    uint32_t* w;       // [kSlotWords][slots]
+    uint32_t slots;
+    __device__ __forceinline__ void bind(uint8_t* base, uint32_t n) {
+        w = reinterpret_cast<uint32_t*>(base);
+        slots = n;
+    }
+    __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
+        for (uint32_t i = tid; i < kSlotWords * slots; i += nthreads) w[i] = 0;
+    }
+    // Rows r of a quad with bit r of `m` set (passing, key < slots, fast domain); atomics first,
+    // carries after.
+    __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
+                                             const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
+        const uint32_t S = slots;
+        uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t a = 100u - d[r];
+            vx[r] = 1u + (d[r] << 24);   // count + 2^24 * discount
+            vd[r] = a * p[r];            // (100 - d) p < 2^31
+            const uint64_t c64 = (uint64_t)(a * (100u + t[r])) * p[r];
+            cl[r] = (uint32_t)c64;
+            ch[r] = (uint32_t)(c64 >> 32);
+            if ((m >> r) & 1u) {
+                const uint32_t s = key[r];
+                ox[r] = atomicAdd(w + s, vx[r]);
+                if (q[r]) atomicAdd(w + 2 * S + s, q[r]);
+                op[r] = atomicAdd(w + 3 * S + s, p[r]);
+                od[r] = atomicAdd(w + 5 * S + s, vd[r]);
+                oc[r] = atomicAdd(w + 7 * S + s, cl[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if ((m >> r) & 1u) {
+                const uint32_t s = key[r];
+                if (ox[r] + vx[r] < ox[r]) atomicAdd(w + S + s, 1u);
+                if (op[r] + p[r] < op[r]) atomicAdd(w + 4 * S + s, 1u);
+                if (od[r] + vd[r] < od[r]) atomicAdd(w + 6 * S + s, 1u);
+                const uint32_t h = ch[r] + (oc[r] + cl[r] < oc[r] ? 1u : 0u);
+                if (h) atomicAdd(w + 8 * S + s, h);
+            }
+        }
+    }
+    __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t tid, uint32_t nthreads) {
+        const uint32_t S = slots;
+        for (uint32_t s = tid; s < S; s += nthreads) {
+            const uint64_t X = ((uint64_t)w[S + s] << 32) | w[s];
+            const uint64_t cnt = X & 0xFFFFFFull;
+            if (cnt) {
+                const uint64_t P = ((uint64_t)w[4 * S + s] << 32) | w[3 * S + s];
+                scratch_add(acc, s, cnt, w[2 * S + s], X >> 24, P, w[5 * S + s], w[6 * S + s], w[7 * S + s],
+                            w[8 * S + s]);
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kSlotWords; ++k) w[k * S + s] = 0;
+        }
+    }
+};
+
+// One quad into a shared table (CubeTable or SlotTable): rows in the table's fast domain go to the
+// table, other passing rows with key < num_groups straight to the scratch, passing rows with
+// key >= num_groups make `bad` nonzero.
+template <class Table>
+__device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_t num_groups, uint32_t hot,
+                                           unsigned long long* acc, uint32_t& bad) {
+    uint32_t q[4], d[4], t[4], m = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        q[r] = (x.Q >> (8 * r)) & 0xFFu;
+        d[r] = (x.D >> (8 * r)) & 0xFFu;
+        t[r] = (x.X >> (8 * r)) & 0xFFu;
+        const bool pass = (x.PM >> (8 * r)) & 1u;
+        const uint32_t key = x.k[r];
+        if (pass && key >= num_groups) bad = 1u;
+        if (pass && key < num_groups) {
+            if (key < hot && fast_domain(d[r], t[r], x.p[r])) m |= 1u << r;
+            else scratch_row(acc, key, q[r], d[r], t[r], x.p[r]);
+        }
+    }
+    if (m) tab.add_quad(m, x.k, q, d, t, x.p);
+}
+
+// Barrier of the consumer warps only (the producer keeps streaming): one arrive per warp on an
+// mbarrier initialised with the warp count, bounded wait. Every consumer passes the same sequence
+// of barriers, so a local phase counter tracks the parity.
+struct ConsumerBarrier {
+    uint32_t addr;
+    uint32_t phase;
+    __device__ __forceinline__ void sync(uint32_t lane, uint32_t* status) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(addr);
+        mbar_wait(addr, phase & 1u, status);
+        ++phase;
+    }
+};
+
+}  // namespace ka
+}  // namespace q1

@@ -28,6 +28,7 @@
 #include "q1_common.cuh"
 #include "q1_kernels.h"
 #include "q1_ptx.cuh"
+#include "q1_quad.cuh"
 
 namespace q1 {
 
@@ -152,81 +153,6 @@ struct GroupRegs {
             case kAggDisc: return kWideQty ? (uint64_t)d32 : (qd64 >> 32);
             case kAggDiscPrice: return dp;
             default: return ch;
-        }
-    }
-};
-
-// Four decoded rows of a compressed tile (a "quad"), handed to a placement at once.
-struct Quad {
-    uint32_t OH;      // byte r: bit g set iff row r passes the predicate and has group code g
-    uint32_t Q, D;    // bytes r: quantity (units) and discount (hundredths) of row r
-    uint32_t a[4];    // 100 - discount
-    uint32_t ab[4];   // (100 - discount) * (100 + tax)
-    uint32_t p[4];    // extendedprice
-    uint32_t A;       // bytes r: 100 - discount
-    uint32_t P[4];    // byte planes of the prices: byte r of P[k] = byte k of p[r]
-    uint32_t ABL, ABH;  // bytes r: low / high byte of ab[r]
-};
-
-// Byte planes of four 32-bit words (a 4x4 byte transpose, eight byte permutes).
-__device__ __forceinline__ void byte_planes(const uint32_t w[4], uint32_t out[4]) {
-    const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140u), t1 = __byte_perm(w[2], w[3], 0x5140u);
-    const uint32_t t2 = __byte_perm(w[0], w[1], 0x7362u), t3 = __byte_perm(w[2], w[3], 0x7362u);
-    out[0] = __byte_perm(t0, t1, 0x5410u);
-    out[1] = __byte_perm(t0, t1, 0x7632u);
-    out[2] = __byte_perm(t2, t3, 0x5410u);
-    out[3] = __byte_perm(t2, t3, 0x7632u);
-}
-
-// Aggregates of one group, per thread, computed with byte dot products (dp4a: four rows per
-// instruction). With W1 = 0/1 bytes of the group's rows and M = its 0x00/0xFF byte mask:
-//   count, qty, disc      dp4a(W1, 1 | Q | D)
-//   sum p                 sum_k 2^8k dp4a(W1, P_k)
-//   sum (100-d) p         sum_k 2^8k dp4a(A & M, P_k)
-//   sum (100-d)(100+t) p  sum_k 2^8k (dp4a(ABL & M, P_k) + 2^8 dp4a(ABH & M, P_k))
-// Every 32-bit partial stays exact while a thread adds at most 2^15 rows per launch (the host
-// caps launches accordingly): the largest, an ab-low plane, grows by <= 4*255*255 per quad.
-struct GroupPlanes {
-    uint32_t cnt, q, d;
-    uint32_t p[4], dp[4], chl[4], chh[4];
-    __device__ __forceinline__ void zero() {
-        cnt = q = d = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) p[k] = dp[k] = chl[k] = chh[k] = 0;
-    }
-    __device__ __forceinline__ void add_quad(uint32_t OH, uint32_t g, const Quad& x) {
-        const uint32_t W1 = (OH >> g) & 0x01010101u;
-        const uint32_t M = (W1 << 8) - W1;   // 0xFF in the group's row bytes
-        const uint32_t MA = x.A & M, ML = x.ABL & M, MH = x.ABH & M;
-        cnt = __dp4a(W1, 0x01010101u, cnt);
-        q = __dp4a(W1, x.Q, q);
-        d = __dp4a(W1, x.D, d);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            p[k] = __dp4a(W1, x.P[k], p[k]);
-            dp[k] = __dp4a(MA, x.P[k], dp[k]);
-            chl[k] = __dp4a(ML, x.P[k], chl[k]);
-            chh[k] = __dp4a(MH, x.P[k], chh[k]);
-        }
-    }
-    __device__ __forceinline__ uint64_t value(int agg) const {
-        uint64_t v = 0;
-        switch (agg) {
-            case kAggCount: return cnt;
-            case kAggQty: return q;
-            case kAggDisc: return d;
-            case kAggBasePrice:
-#pragma unroll
-                for (int k = 0; k < 4; ++k) v += (uint64_t)p[k] << (8 * k);
-                return v;
-            case kAggDiscPrice:
-#pragma unroll
-                for (int k = 0; k < 4; ++k) v += (uint64_t)dp[k] << (8 * k);
-                return v;
-            default:
-#pragma unroll
-                for (int k = 0; k < 4; ++k) v += ((uint64_t)chl[k] << (8 * k)) + ((uint64_t)chh[k] << (8 * k + 8));
-                return v;
         }
     }
 };
@@ -533,10 +459,6 @@ template <int G, bool W> struct AccSel<kPlaceGlobal, G, W> { using T = AccGlobal
 // Row decoding
 // ---------------------------------------------------------------------------------------------
 
-// Any byte of a discount word above 100 (top bit of (b & 0x7F) + 27, or b >= 128).
-__device__ __forceinline__ uint32_t disc_out_of_domain4(uint32_t D) {
-    return (((D & 0x7F7F7F7Fu) + 0x1B1B1B1Bu) | D) & 0x80808080u;
-}
 
 __device__ __forceinline__ uint32_t code_of_chars(uint32_t rf, uint32_t ls) {
     const uint32_t r = (rf == 'R' ? 2u : 0u) + (rf == 'N' ? 1u : 0u);
@@ -579,12 +501,7 @@ __device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t 
             const uint32_t bits = (lds_u8(base + col_offset<L>(0, R) + (j >> 1)) >> ((j & 1u) * 4u)) & 0xFu;
             PM = ((bits * 0x00204081u) & 0x01010101u) * 0xFFu;
         } else {
-            // Two 16-bit lanes per subtraction: lane = (cut + 2^15) - ship has its top bit set iff
-            // ship <= cut; no borrow crosses lanes for ship <= 32767 and -1 <= cut <= 32767.
-            const uint2 sd = lds_v2(base + col_offset<L>(0, R) + 8 * j);
-            const uint32_t c2 = (uint32_t)(cut + 32768) * 0x00010001u;
-            bad |= (sd.x | sd.y) & 0x80008000u;   // ship offset above 32767: outside the domain
-            PM = prmt(c2 - sd.x, c2 - sd.y, 0xFDB9u);
+            PM = quad_pass_mask(lds_v2(base + col_offset<L>(0, R) + 8 * j), cut, bad);
         }
         Quad x;
         x.Q = lds_u32(base + col_offset<L>(1, R) + 4 * j);
@@ -602,23 +519,11 @@ __device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t 
             OH = (OH + (OH & lsm)) & 0x3F3F3F3Fu;
         }
         x.OH = OH & PM;
-        const uint32_t A = 0x64646464u - x.D;   // 100 - d per byte (no borrow inside the domain)
-        x.A = A;
         x.p[0] = P.x;
         x.p[1] = P.y;
         x.p[2] = P.z;
         x.p[3] = P.w;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            x.a[r] = __byte_perm(A, 0u, 0x4440u | (uint32_t)r);
-            x.ab[r] = x.a[r] * (100u + __byte_perm(X, 0u, 0x4440u | (uint32_t)r));
-        }
-        byte_planes(x.p, x.P);
-        {
-            const uint32_t u = __byte_perm(x.ab[0], x.ab[1], 0x5140u), v = __byte_perm(x.ab[2], x.ab[3], 0x5140u);
-            x.ABL = __byte_perm(u, v, 0x5410u);
-            x.ABH = __byte_perm(u, v, 0x7632u);
-        }
+        quad_derive(x, X);
         acc.add_quad(x);
     }
 }
