@@ -212,7 +212,14 @@ q1_status validate_request(const q1_request* r, uint64_t max_adhoc_rows, uint64_
     return Q1_OK;
 }
 
+// Group slots of a response: the 6 (returnflag, linestatus) groups or the request's key groups.
 inline uint32_t groups_of(const q1_request& r) { return r.grouping == Q1_GROUP_FLAGS ? 6u : r.num_groups; }
+
+// Key values of an ad-hoc table: its (returnflag, linestatus) dictionary codes (AF, NF, NO, RF)
+// or the request's key groups. Code c belongs to group kPairGroup[c].
+constexpr uint32_t kPairGroup[4] = {0, 2, 3, 4};
+inline bool coded(const q1_request& r) { return r.kind == Q1_REQ_ADHOC && r.grouping == Q1_GROUP_FLAGS; }
+inline uint32_t key_groups(const q1_request& r) { return coded(r) ? 4u : groups_of(r); }
 
 inline int32_t cutoff_rel(int32_t cutoff_day) {
     const int64_t rel = (int64_t)cutoff_day - kShipDateFrame;
@@ -448,13 +455,14 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
         BatchInstanceDev& d = inst[ninst];
         memset(&d, 0, sizeof(d));
         for (int c = 0; c < 6; ++c) d.col[c] = tp.base + tp.L.off[c];
+        const uint32_t kg = key_groups(t->req);
         d.rows = t->req.adhoc_rows;
         d.cutoff = cut;
-        d.num_groups = t->groups;
-        d.mode = t->groups <= 4 ? kModeRegisters : kModeShared;
+        d.num_groups = kg;
+        d.mode = kg <= 4 ? kModeRegisters : kModeShared;
         d.acc = s->d_scratch.as<unsigned long long>() + 8 * groups;
         d.out = s->d_resp.as<unsigned long long>() + (uint64_t)i * kRespWords;
-        groups += t->groups;
+        groups += kg;
         base[ninst + 1] = groups;
         tiles += (d.rows + kBatchTileRows - 1) / kBatchTileRows;
         ++ninst;
@@ -501,9 +509,8 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
 // The plain launch of one request over device columns: the drop-in Q1 scan for the
 // (returnflag, linestatus) grouping of pair-coded columns, else the group-key scan. Accumulates
 // into `out` (caller-zeroed int128 [groups][6]).
-q1_status plain_launch(const q1_request& req, const q1_compressed_columns& c, const uint32_t* keys, uint64_t rows,
-                       void* scratch, q1_i128* out, cudaStream_t sm) {
-    const uint32_t G = groups_of(req);
+q1_status plain_launch(const q1_request& req, const q1_compressed_columns& c, const uint32_t* keys, uint32_t G,
+                       uint64_t rows, void* scratch, q1_i128* out, cudaStream_t sm) {
     if (c.flags && !keys)
         return q1_launch_compressed(Q1_PLACEMENT_IN_REGISTERS_PER_THREAD, &c, rows, req.cutoff_day, 0, nullptr, out, sm);
     return q1_launch_groupkey(G <= 8 ? Q1_PLACEMENT_IN_REGISTERS_PER_THREAD : Q1_PLACEMENT_SHARED_MEM_PER_THREAD, &c,
@@ -533,8 +540,9 @@ q1_status enqueue_plain(q1_server* s, Ticket* t) {
         keys = reinterpret_cast<const uint32_t*>(tp.base + tp.L.off[5]);
         rows = t->req.adhoc_rows;
     }
-    if ((r = plain_launch(t->req, c, keys, rows, s->plain_scratch.p, s->d_resp.as<q1_i128>(), st)) != Q1_OK) return r;
-    Q1_CUDA(cudaMemcpyAsync(s->h_resp.p, s->d_resp.p, (uint64_t)t->groups * 12 * 8, cudaMemcpyDeviceToHost, st));
+    const uint32_t G = t->req.kind == Q1_REQ_RESIDENT ? t->groups : key_groups(t->req);
+    if ((r = plain_launch(t->req, c, keys, G, rows, s->plain_scratch.p, s->d_resp.as<q1_i128>(), st)) != Q1_OK) return r;
+    Q1_CUDA(cudaMemcpyAsync(s->h_resp.p, s->d_resp.p, (uint64_t)G * 12 * 8, cudaMemcpyDeviceToHost, st));
     return Q1_OK;
 }
 
@@ -550,10 +558,20 @@ void run_round(q1_server* s, const std::vector<Ticket*>& batch) {
     for (size_t i = 0; i < batch.size(); ++i) {
         Ticket* t = batch[i];
         if (r == Q1_OK) {
-            t->aggs.resize((size_t)t->groups * 6);
-            for (uint32_t w = 0; w < t->groups * 6; ++w) {
-                t->aggs[w].lo = words[i * kRespWords + 2 * w];
-                t->aggs[w].hi = words[i * kRespWords + 2 * w + 1];
+            const unsigned long long* src = words + i * kRespWords;
+            t->aggs.assign((size_t)t->groups * 6, q1_i128{0, 0});
+            if (coded(t->req)) {
+                // table keys are dictionary codes: code c holds group kPairGroup[c]
+                for (uint32_t c = 0; c < 4; ++c)
+                    for (uint32_t a = 0; a < 6; ++a) {
+                        t->aggs[kPairGroup[c] * 6 + a].lo = src[12 * c + 2 * a];
+                        t->aggs[kPairGroup[c] * 6 + a].hi = src[12 * c + 2 * a + 1];
+                    }
+            } else {
+                for (uint32_t w = 0; w < t->groups * 6; ++w) {
+                    t->aggs[w].lo = src[2 * w];
+                    t->aggs[w].hi = src[2 * w + 1];
+                }
             }
         }
         if (t->table) {
@@ -798,7 +816,8 @@ q1_status q1_server_plain(q1_server* s, const q1_request* req, q1_response* out)
             keys = reinterpret_cast<const uint32_t*>(tb + L.off[5]);
         }
     }
-    if ((st = plain_launch(*req, c, keys, rows, s->judge_scratch.p, s->judge_out.as<q1_i128>(), sm)) != Q1_OK) return st;
+    if ((st = plain_launch(*req, c, keys, G, rows, s->judge_scratch.p, s->judge_out.as<q1_i128>(), sm)) != Q1_OK)
+        return st;
     std::vector<unsigned long long> words((size_t)G * 12);
     Q1_CUDA(cudaMemcpyAsync(words.data(), s->judge_out.p, (size_t)G * 12 * 8, cudaMemcpyDeviceToHost, sm));
     if ((st = check_device_status(sm, s->di->status)) != Q1_OK) return st;

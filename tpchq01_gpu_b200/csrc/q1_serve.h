@@ -15,7 +15,8 @@ struct KeyedTableOut {
     uint32_t* keys;
 };
 
-// pair_keys != 0: key = (rf << 1) + ls of the row; otherwise uniform in [0, num_groups).
+// pair_keys != 0: key = the dictionary code of the row's (rf, ls) pair (AF, NF, NO, RF = 0..3);
+// otherwise uniform in [0, num_groups).
 cudaError_t launch_generate_keyed_table(uint64_t seed, uint64_t rows, uint32_t pair_keys, uint32_t num_groups,
                                         const KeyedTableOut& out, cudaStream_t stream);
 

@@ -1,7 +1,8 @@
 // Kernels of the serving loop (q1_serve.cpp):
 //   * generate_keyed_table: an ad-hoc group-key table (ship u16, qty u8, disc u8, tax u8,
-//     price u32, key u32) from the seeded generator; key = (rf << 1) + ls ("pair" keys, the Q1
-//     groups) or a uniform key in [0, G);
+//     price u32, key u32) from the seeded generator; key = the row's (returnflag, linestatus)
+//     dictionary code (0..3 for AF, NF, NO, RF: "pair" keys, the Q1 groups) or a uniform key in
+//     [0, G);
 //   * cube_pass: partial aggregates per (ship day, group) for a window of days of the resident
 //     table, reduced into split-limb scratch (one shared-memory table per CTA);
 //   * cube_finalize / cube_prefix: scratch -> int128 cube, then prefix sums over days, so that the
@@ -29,7 +30,7 @@ __global__ void __launch_bounds__(256) generate_keyed_table_kernel(uint64_t key,
     out.discount[i] = (uint8_t)g.discount;
     out.tax[i] = (uint8_t)g.tax;
     out.extendedprice[i] = g.extprice;
-    out.keys[i] = pair_keys ? group_of(encode_return_flag(g.returnflag), encode_line_status(g.linestatus))
+    out.keys[i] = pair_keys ? gen_pair_code(group_of(encode_return_flag(g.returnflag), encode_line_status(g.linestatus)))
                             : gen_group_key_uniform(key, i, num_groups);
 }
 
