@@ -405,24 +405,46 @@ def main():
 
 
 def e2e_pinned(q, args):
-    """Same workload through the public API with host buffers: q1_run on a pinned-host table."""
-    ctx = q.Q1Context()
+    """Same workload through the public API with host buffers: q1_run on a pinned-host table with
+    the reference's own options --use-filter-pushdown --use-coprocessing: host threads build the
+    predicate bitmap for the GPU's share (7.375 B/row cross PCIe instead of 9.25) and aggregate
+    the CPU's share, merged exactly. The CPU fraction is picked from a short sweep during warm-up."""
+    threads = max(1, (os.cpu_count() or 2) - 2)
+    ctx = q.Q1Context(cpu_threads=threads)
     try:
         ctx.generate(SEED, ROWS, layout="compressed", packing="pair", residency="pinned")
-        p = q.Q1Params(hash_table_placement=args.placement, apply_compression=True, num_gpu_streams=4,
-                       num_tuples_per_kernel_launch=1 << 24, num_query_execution_runs=1, cutoff_day=CUTOFF)
-        for _ in range(max(1, min(args.warmup, 2))):
-            ctx.run(p)
+
+        def params(frac):
+            return q.Q1Params(hash_table_placement=args.placement, apply_compression=True, use_filter_pushdown=True,
+                              use_coprocessing=True, cpu_processing_fraction=frac, num_gpu_streams=4,
+                              num_tuples_per_kernel_launch=1 << 24, num_query_execution_runs=1, cutoff_day=CUTOFF)
+
+        def timed(p, n):
+            t = []
+            for _ in range(n):
+                s = time.perf_counter()
+                ctx.run(p)
+                t.append(time.perf_counter() - s)
+            return t
+
+        sweep = {}
+        frac, worse = 0.25, 0
+        while frac < 0.86 and worse < 2:   # climb until two steps in a row are slower
+            timed(params(frac), 1)
+            sweep[frac] = min(timed(params(frac), 2))
+            worse = worse + 1 if sweep[frac] > min(sweep.values()) else 0
+            frac = round(frac + 0.05, 2)
+        best = min(sweep, key=sweep.get)
         steps = max(3, min(args.steps, 10))
-        t = []
-        for _ in range(steps):
-            s = time.perf_counter()
-            ctx.run(p)
-            t.append(time.perf_counter() - s)
-        h2d = int(ROWS * 2 + ROWS * 3 + ROWS * 4 + 4 * ((ROWS + 15) // 16))
+        t = timed(params(best), steps)
+        gpu_rows = int(ROWS * (1 - best))
+        h2d = int(gpu_rows * 3 + gpu_rows * 4 + 4 * ((gpu_rows + 31) // 32) + 4 * ((gpu_rows + 15) // 16))
         return {"value": ROWS * steps / sum(t), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 576,
                 "steps": steps, "ms_per_step": 1000 * sum(t) / steps,
-                "path": "q1_run, PINNED_HOST residency, 4 streams x 16M-row chunks (H2D + scan per chunk)"}
+                "path": "q1_run, PINNED_HOST residency, use_filter_pushdown + use_coprocessing, 4 streams x 16M-row "
+                        "chunks (H2D + scan per chunk), host predicate bitmap and CPU share on "
+                        f"{threads} threads",
+                "cpu_fraction": best, "cpu_fraction_sweep_ms": {str(k): 1000 * v for k, v in sweep.items()}}
     finally:
         ctx.close()
 

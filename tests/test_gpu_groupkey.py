@@ -93,7 +93,7 @@ def check(comp, keys, num_groups, cutoff, got):
 CUTOFFS = [727600, 728660, 729999, 730089]
 
 
-@pytest.mark.parametrize("num_groups", [4, 64, 1024, 65536])
+@pytest.mark.parametrize("num_groups", [4, 64, 65, 1024, 65536])
 @pytest.mark.parametrize("dist", ["uniform", "zipf"])
 @pytest.mark.parametrize("placement", ["shared_mem_per_thread", "global"])
 def test_groupkey_placements(table, num_groups, dist, placement):
@@ -137,7 +137,7 @@ def long_table(cuda):
 
 @pytest.mark.parametrize("num_groups,placement", [
     (4, "in_registers_per_thread"), (8, "in_registers_per_thread"), (64, "shared_mem_per_thread"),
-    (1024, "shared_mem_per_thread"), (5000, "shared_mem_per_thread")])
+    (200, "shared_mem_per_thread"), (1024, "shared_mem_per_thread"), (5000, "shared_mem_per_thread")])
 def test_one_cta_flushes_mid_launch(long_table, num_groups, placement):
     """One CTA over 9M rows: the per-thread planes (every 4032 tiles) and the shared tables
     (every 2^23 rows) are flushed inside the launch."""

@@ -16,8 +16,9 @@
 // instance changes they flush their accumulators into the instance's scratch (red.global.add),
 // according to the instance's placement mode:
 //   kModeRegisters  num_groups <= 4: per-thread dp4a byte planes (ka::PlaneRegs<4>)
-//   kModeShared     num_groups <= 256: shared (group, discount) cells (ka::CubeTable); more
-//                   groups: shared slots for keys < 2048 (ka::SlotTable), the rest spilled
+//   kModeShared     num_groups <= 64: shared (group, discount, tax) cells (ka::Cube3Table);
+//                   <= 256: shared (group, discount) cells (ka::CubeTable); more groups:
+//                   shared slots for keys < 2048 (ka::SlotTable), the rest spilled
 //   kModeGlobal     every passing row reduces straight into the scratch accumulators
 // (engines in q1_keyagg.cuh). Scratch per instance: num_groups x 8 u64, folded into the
 // caller's int128 table by batch_finalize.
@@ -43,8 +44,9 @@ constexpr uint32_t kStage = ka::kStageBytes;
 constexpr uint32_t kSteps = R / 4;
 constexpr uint32_t kKindFull = 0, kKindPartial = 1, kKindEnd = 2;
 // shared table region: the larger of the cube (256 groups) and the slot table (2048 slots)
+constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 constexpr uint32_t kTableBytes =
-    ka::cube_bytes(ka::kCubeMaxGroups) > ka::slot_bytes(ka::kSlots) ? ka::cube_bytes(ka::kCubeMaxGroups) : ka::slot_bytes(ka::kSlots);
+    cmax(ka::cube3_bytes(ka::kCube3MaxGroups), cmax(ka::cube_bytes(ka::kCubeMaxGroups), ka::slot_bytes(ka::kSlots)));
 
 struct StageMeta {
     uint32_t instance;
@@ -134,12 +136,14 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
         uint32_t cur = 0xFFFFFFFFu;
         BatchInstanceDev in{};
         uint32_t mode = kModeGlobal;
-        bool use_cube = false;
+        uint32_t table = 0;   // 0 slots, 1 (group, discount) cube, 2 (group, discount, tax) cube
         uint32_t hot = 0;
         ka::PlaneRegs<4> regs;
         regs.zero();
+        ka::Cube3Table cube3;
         ka::CubeTable cube;
         ka::SlotTable slots;
+        cube3.bind(tab, 0);
         cube.bind(tab, 0);
         slots.bind(tab, 0);
         ka::ConsumerBarrier cb{smem_addr(&consumers_bar), 0};
@@ -158,7 +162,8 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
                 regs.flush(in.acc, in.num_groups, lane);
             } else if (mode == kModeShared) {
                 cb.sync(lane, prm.status);
-                if (use_cube) cube.flush(in.acc, in.num_groups, ctid, W * 32);
+                if (table == 2) cube3.flush(in.acc, in.num_groups, ctid, W * 32);
+                else if (table == 1) cube.flush(in.acc, in.num_groups, ctid, W * 32);
                 else slots.flush(in.acc, ctid, W * 32);
                 cb.sync(lane, prm.status);
             }
@@ -167,7 +172,8 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
             if (mode == kModeRegisters) {
                 regs.add(x, in.num_groups, bad);
             } else if (mode == kModeShared) {
-                if (use_cube) ka::table_quad(cube, x, in.num_groups, hot, in.acc, bad);
+                if (table == 2) ka::table_quad(cube3, x, in.num_groups, hot, in.acc, bad);
+                else if (table == 1) ka::table_quad(cube, x, in.num_groups, hot, in.acc, bad);
                 else ka::table_quad(slots, x, in.num_groups, hot, in.acc, bad);
             } else {
 #pragma unroll
@@ -197,9 +203,10 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
                 in = prm.inst[cur];
                 mode = in.mode;
                 if (mode == kModeRegisters && in.num_groups > 4) mode = kModeShared;   // planes hold 4 groups
-                use_cube = in.num_groups <= ka::kCubeMaxGroups;
-                hot = use_cube ? in.num_groups : (in.num_groups < ka::kSlots ? in.num_groups : ka::kSlots);
-                if (use_cube) cube.bind(tab, in.num_groups);
+                table = in.num_groups <= ka::kCube3MaxGroups ? 2u : (in.num_groups <= ka::kCubeMaxGroups ? 1u : 0u);
+                hot = table ? in.num_groups : (in.num_groups < ka::kSlots ? in.num_groups : ka::kSlots);
+                if (table == 2) cube3.bind(tab, in.num_groups);
+                else if (table == 1) cube.bind(tab, in.num_groups);
                 else slots.bind(tab, hot);
             } else if ((mode == kModeRegisters && tiles_since >= ka::kPlaneFlushTiles) ||
                        (mode == kModeShared && rows_since + m.rows > ka::kTableFlushRows)) {

@@ -10,7 +10,8 @@
 //
 // Placements:
 //   in_registers_per_thread  num_groups <= 8: per-thread dp4a byte planes (PlaneRegs<4|8>)
-//   shared_mem_per_thread    num_groups <= 256: shared (group, discount) cells (CubeTable);
+//   shared_mem_per_thread    num_groups <= 64: shared (group, discount, tax) cells
+//                            (Cube3Table); <= 256: shared (group, discount) cells (CubeTable);
 //                            otherwise keys < 2048 in shared slots (SlotTable), larger keys
 //                            reduced straight into the global accumulators
 //   global                   every passing row reduces into the global accumulators
@@ -42,16 +43,21 @@ static_assert(kSteps % (W * 32) == 0, "steps must divide evenly");
 static_assert(kStage % 16 == 0, "stage alignment");
 
 // Table engine of the shared_mem_per_thread placement.
-enum TableKind : uint32_t { kTableNone = 0, kTableCube = 1, kTableSlots = 2 };
+enum TableKind : uint32_t { kTableNone = 0, kTableCube = 1, kTableSlots = 2, kTableCube3 = 3 };
 
 __host__ __device__ constexpr uint32_t table_kind(int placement, uint32_t num_groups) {
-    return placement != kPlaceSharedMemPerThread ? kTableNone
-                                                 : (num_groups <= ka::kCubeMaxGroups ? kTableCube : kTableSlots);
+    return placement != kPlaceSharedMemPerThread
+               ? kTableNone
+               : (num_groups <= ka::kCube3MaxGroups ? kTableCube3
+                                                    : (num_groups <= ka::kCubeMaxGroups ? kTableCube : kTableSlots));
 }
 __host__ __device__ constexpr uint32_t table_bytes(uint32_t kind, uint32_t num_groups) {
-    return kind == kTableCube ? ka::cube_bytes(num_groups)
-                              : (kind == kTableSlots ? ka::slot_bytes(num_groups < ka::kSlots ? num_groups : ka::kSlots)
-                                                     : 0u);
+    return kind == kTableCube3 ? ka::cube3_bytes(num_groups)
+                               : (kind == kTableCube ? ka::cube_bytes(num_groups)
+                                                     : (kind == kTableSlots ? ka::slot_bytes(num_groups < ka::kSlots
+                                                                                                 ? num_groups
+                                                                                                 : ka::kSlots)
+                                                                            : 0u));
 }
 
 }  // namespace gk
@@ -79,11 +85,13 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
     const uint64_t num_tiles = prm.rows / R;
     const uint32_t ring = smem_addr(smem);
     const uint32_t G = prm.num_groups;
+    ka::Cube3Table cube3;
     ka::CubeTable cube;
     ka::SlotTable slots;
     const uint32_t hot = G < ka::kSlots ? G : ka::kSlots;
     if (P == kPlaceSharedMemPerThread) {
-        if (prm.table == kTableCube) cube.bind(smem + S * kStage, G);
+        if (prm.table == kTableCube3) cube3.bind(smem + S * kStage, G);
+        else if (prm.table == kTableCube) cube.bind(smem + S * kStage, G);
         else slots.bind(smem + S * kStage, hot);
     }
 
@@ -96,7 +104,8 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
         fence_mbar_init();
     }
     if (P == kPlaceSharedMemPerThread) {
-        if (prm.table == kTableCube) cube.zero(threadIdx.x, blockDim.x);
+        if (prm.table == kTableCube3) cube3.zero(threadIdx.x, blockDim.x);
+        else if (prm.table == kTableCube) cube.zero(threadIdx.x, blockDim.x);
         else slots.zero(threadIdx.x, blockDim.x);
     }
     __syncthreads();
@@ -131,7 +140,8 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
             if constexpr (P == kPlaceInRegistersPerThread) {
                 regs.add(x, G, bad);
             } else if constexpr (P == kPlaceSharedMemPerThread) {
-                if (prm.table == kTableCube) ka::table_quad(cube, x, G, G, prm.acc, bad);
+                if (prm.table == kTableCube3) ka::table_quad(cube3, x, G, G, prm.acc, bad);
+                else if (prm.table == kTableCube) ka::table_quad(cube, x, G, G, prm.acc, bad);
                 else ka::table_quad(slots, x, G, hot, prm.acc, bad);
             } else {
 #pragma unroll
@@ -149,7 +159,8 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
         };
         auto table_flush = [&]() {
             cb.sync(lane, prm.status);
-            if (prm.table == kTableCube) cube.flush(prm.acc, G, ctid, W * 32);
+            if (prm.table == kTableCube3) cube3.flush(prm.acc, G, ctid, W * 32);
+            else if (prm.table == kTableCube) cube.flush(prm.acc, G, ctid, W * 32);
             else slots.flush(prm.acc, ctid, W * 32);
             cb.sync(lane, prm.status);
         };
@@ -191,7 +202,8 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
     }
     __syncthreads();
     if (P == kPlaceSharedMemPerThread) {
-        if (prm.table == kTableCube) cube.flush(prm.acc, G, threadIdx.x, blockDim.x);
+        if (prm.table == kTableCube3) cube3.flush(prm.acc, G, threadIdx.x, blockDim.x);
+        else if (prm.table == kTableCube) cube.flush(prm.acc, G, threadIdx.x, blockDim.x);
         else slots.flush(prm.acc, threadIdx.x, blockDim.x);
     }
 }

@@ -4,6 +4,8 @@
 // behind CoProc (src/cpu.cpp:13-69) and hands filter chunks to the GPU loop through a moodycamel
 // queue (src/cpu.h:12-21). This file is this project's own equivalent: a fixed thread pool with
 // an atomic morsel cursor supplied by the caller, an exact 128-bit merge, and a blocking queue.
+#include <immintrin.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -146,7 +148,96 @@ inline void add_row(Partial& p, uint32_t g, uint64_t q, uint64_t d, uint64_t t, 
 
 }  // namespace
 
+namespace {
+
+// Pair layout, 16 rows per step with AVX-512: the 2-bit codes of a 16-row word become per-code
+// lane masks; count, quantity and discount add in 32-bit lanes, price, (100-d) p and
+// (100-d)(100+t) p in 64-bit lanes (products of 32-bit lanes, exact). Every lane sum stays
+// exact within a block of kBlock rows. Rows [begin, end) with begin and end multiples of 16.
+__attribute__((target("avx512f,avx512bw,avx512dq"))) bool aggregate_pair_avx512(const HostCompressed& t,
+                                                                                 uint64_t begin, uint64_t end,
+                                                                                 int32_t cutoff_rel, Agg128* out) {
+    const __m512i shifts = _mm512_setr_epi32(0, 2, 4, 6, 8, 10, 12, 14, 16, 18, 20, 22, 24, 26, 28, 30);
+    const __m512i three = _mm512_set1_epi32(3), one = _mm512_set1_epi32(1), hundred = _mm512_set1_epi32(100);
+    const __m512i cut = _mm512_set1_epi32(cutoff_rel);
+    bool ok = true;
+    for (uint64_t b0 = begin; b0 < end; b0 += kBlock) {
+        const uint64_t b1 = std::min(end, b0 + kBlock);
+        __m512i cnt[4], q[4], d[4], p[4][2], dp[4][2], ch[4][2];
+        for (int k = 0; k < 4; ++k) {
+            cnt[k] = q[k] = d[k] = _mm512_setzero_si512();
+            for (int h = 0; h < 2; ++h) p[k][h] = dp[k][h] = ch[k][h] = _mm512_setzero_si512();
+        }
+        __mmask16 bad = 0;
+        for (uint64_t i = b0; i < b1; i += 16) {
+            const __m512i ship = _mm512_cvtepu16_epi32(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(t.ship + i)));
+            const __mmask16 pass = _mm512_cmple_epi32_mask(ship, cut);
+            const __m512i code = _mm512_and_si512(_mm512_srlv_epi32(_mm512_set1_epi32((int)t.flags[i >> 4]), shifts), three);
+            const __m512i vq = _mm512_cvtepu8_epi32(_mm_loadu_si128(reinterpret_cast<const __m128i*>(t.qty + i)));
+            const __m512i vd = _mm512_cvtepu8_epi32(_mm_loadu_si128(reinterpret_cast<const __m128i*>(t.disc + i)));
+            const __m512i vt = _mm512_cvtepu8_epi32(_mm_loadu_si128(reinterpret_cast<const __m128i*>(t.tax + i)));
+            const __m512i vp = _mm512_loadu_si512(t.price + i);
+            bad |= _mm512_mask_cmpgt_epu32_mask(pass, vd, hundred);
+            const __m512i a = _mm512_sub_epi32(hundred, vd);
+            const __m512i ab = _mm512_mullo_epi32(a, _mm512_add_epi32(hundred, vt));
+            // 64-bit lanes: rows 0-7 (h = 0) and 8-15 (h = 1)
+            __m512i p64[2], a64[2], ab64[2];
+            p64[0] = _mm512_cvtepu32_epi64(_mm512_castsi512_si256(vp));
+            p64[1] = _mm512_cvtepu32_epi64(_mm512_extracti64x4_epi64(vp, 1));
+            a64[0] = _mm512_cvtepu32_epi64(_mm512_castsi512_si256(a));
+            a64[1] = _mm512_cvtepu32_epi64(_mm512_extracti64x4_epi64(a, 1));
+            ab64[0] = _mm512_cvtepu32_epi64(_mm512_castsi512_si256(ab));
+            ab64[1] = _mm512_cvtepu32_epi64(_mm512_extracti64x4_epi64(ab, 1));
+            __m512i dp64[2], ch64[2];
+            for (int h = 0; h < 2; ++h) {
+                dp64[h] = _mm512_mul_epu32(a64[h], p64[h]);
+                ch64[h] = _mm512_mul_epu32(ab64[h], p64[h]);
+            }
+            for (int k = 0; k < 4; ++k) {
+                const __mmask16 m = pass & _mm512_cmpeq_epi32_mask(code, _mm512_set1_epi32(k));
+                cnt[k] = _mm512_mask_add_epi32(cnt[k], m, cnt[k], one);
+                q[k] = _mm512_mask_add_epi32(q[k], m, q[k], vq);
+                d[k] = _mm512_mask_add_epi32(d[k], m, d[k], vd);
+                const __mmask8 m0 = (__mmask8)(m & 0xFF), m1 = (__mmask8)(m >> 8);
+                p[k][0] = _mm512_mask_add_epi64(p[k][0], m0, p[k][0], p64[0]);
+                p[k][1] = _mm512_mask_add_epi64(p[k][1], m1, p[k][1], p64[1]);
+                dp[k][0] = _mm512_mask_add_epi64(dp[k][0], m0, dp[k][0], dp64[0]);
+                dp[k][1] = _mm512_mask_add_epi64(dp[k][1], m1, dp[k][1], dp64[1]);
+                ch[k][0] = _mm512_mask_add_epi64(ch[k][0], m0, ch[k][0], ch64[0]);
+                ch[k][1] = _mm512_mask_add_epi64(ch[k][1], m1, ch[k][1], ch64[1]);
+            }
+        }
+        ok &= bad == 0;
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t g = t.pair_group[k];
+            if (g >= 6) continue;
+            u128* r = out->v[g];
+            r[kAggCount] += (uint64_t)_mm512_reduce_add_epi32(cnt[k]);
+            r[kAggQty] += (uint64_t)(uint32_t)_mm512_reduce_add_epi32(q[k]) * 100u;
+            r[kAggDisc] += (uint64_t)(uint32_t)_mm512_reduce_add_epi32(d[k]);
+            r[kAggBasePrice] += (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(p[k][0], p[k][1]));
+            r[kAggDiscPrice] += (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(dp[k][0], dp[k][1]));
+            r[kAggCharge] += (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(ch[k][0], ch[k][1]));
+        }
+    }
+    return ok;
+}
+
+}  // namespace
+
 bool cpu_aggregate_compressed(const HostCompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_rel, Agg128* out) {
+    static const bool avx512 = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
+                               __builtin_cpu_supports("avx512dq");
+    if (avx512 && t.pair && end - begin >= 64) {
+        // scalar head and tail around a 16-aligned body
+        const uint64_t b = std::min<uint64_t>(end, (begin + 15) & ~(uint64_t)15);
+        const uint64_t e = std::max<uint64_t>(b, end & ~(uint64_t)15);
+        bool ok = true;
+        if (begin < b) ok &= cpu_aggregate_compressed(t, begin, b, cutoff_rel, out);
+        if (b < e) ok &= aggregate_pair_avx512(t, b, e, cutoff_rel, out);
+        if (e < end) ok &= cpu_aggregate_compressed(t, e, end, cutoff_rel, out);
+        return ok;
+    }
     Partial part;
     bool ok = true;
     for (uint64_t b0 = begin; b0 < end; b0 += kBlock) {
@@ -191,13 +282,45 @@ bool cpu_aggregate_uncompressed(const HostUncompressed& t, uint64_t begin, uint6
     return ok;
 }
 
-void cpu_precompute_filter(const uint16_t* ship, uint64_t begin, uint64_t end, int32_t cutoff_rel, uint32_t* bitmap) {
-    for (uint64_t w0 = begin; w0 < end; w0 += 32) {
-        uint32_t bits = 0;
-        const uint64_t n = std::min<uint64_t>(32, end - w0);
-        for (uint64_t j = 0; j < n; ++j) bits |= (uint32_t)((int32_t)ship[w0 + j] <= cutoff_rel) << j;
-        bitmap[w0 / 32] = bits;
+namespace {
+
+uint32_t filter_word_scalar(const uint16_t* ship, uint64_t n, int32_t cutoff_rel) {
+    uint32_t bits = 0;
+    for (uint64_t j = 0; j < n; ++j) bits |= (uint32_t)((int32_t)ship[j] <= cutoff_rel) << j;
+    return bits;
+}
+
+// 32 ship offsets per step with AVX2: two signed 16-bit compares against the cutoff, a pack and a
+// byte movemask. Offsets above 32767 (outside the compressed domain) read as negative int16, so
+// such a word is redone by the scalar loop.
+__attribute__((target("avx2"))) void filter_avx2(const uint16_t* ship, uint64_t begin, uint64_t end,
+                                                  int32_t cutoff_rel, uint32_t* bitmap) {
+    const int16_t cut = (int16_t)std::max(-1, std::min(32767, cutoff_rel));
+    const __m256i vcut = _mm256_set1_epi16(cut);
+    const __m256i zero = _mm256_setzero_si256();
+    uint64_t w0 = begin;
+    for (; w0 + 32 <= end; w0 += 32) {
+        const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(ship + w0));
+        const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(ship + w0 + 16));
+        const __m256i gt = _mm256_permute4x64_epi64(
+            _mm256_packs_epi16(_mm256_cmpgt_epi16(a, vcut), _mm256_cmpgt_epi16(b, vcut)), 0xD8);
+        const __m256i neg = _mm256_packs_epi16(_mm256_cmpgt_epi16(zero, a), _mm256_cmpgt_epi16(zero, b));
+        if (_mm256_movemask_epi8(neg)) bitmap[w0 / 32] = filter_word_scalar(ship + w0, 32, cutoff_rel);
+        else bitmap[w0 / 32] = ~(uint32_t)_mm256_movemask_epi8(gt);
     }
+    if (w0 < end) bitmap[w0 / 32] = filter_word_scalar(ship + w0, end - w0, cutoff_rel);
+}
+
+}  // namespace
+
+void cpu_precompute_filter(const uint16_t* ship, uint64_t begin, uint64_t end, int32_t cutoff_rel, uint32_t* bitmap) {
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    if (avx2) {
+        filter_avx2(ship, begin, end, cutoff_rel, bitmap);
+        return;
+    }
+    for (uint64_t w0 = begin; w0 < end; w0 += 32)
+        bitmap[w0 / 32] = filter_word_scalar(ship + w0, std::min<uint64_t>(32, end - w0), cutoff_rel);
 }
 
 }  // namespace q1

@@ -7,6 +7,8 @@
 // Engines (one per placement):
 //   PlaneRegs<NG>  num_groups <= NG (4 or 8): per-thread byte-plane dot products (dp4a), four
 //                  rows per instruction, as in the scan kernel; no atomics until a flush.
+//   Cube3Table     num_groups <= 64: a shared-memory table per (group, discount, tax) cell; a
+//                  row adds its count and quantity (one packed word) and its price: two atomics.
 //   CubeTable      num_groups <= 256: a shared-memory table per (group, discount) cell. A row
 //                  adds only its count and quantity (one packed word), its price and tax * price;
 //                  the discounted sums follow exactly at the flush, because the discount of a
@@ -58,10 +60,16 @@ constexpr uint64_t kTableFlushRows = 1ull << 23;
 constexpr uint32_t kCubeMaxGroups = 256;
 constexpr uint32_t kCubeDisc = 11;          // discount 0..10
 constexpr uint32_t kCubeWords = 6;          // xlo xhi plo phi tlo thi
+constexpr uint32_t kCube3MaxGroups = 64;
+constexpr uint32_t kCubeTax = 9;            // tax 0..8
+constexpr uint32_t kCube3Words = 4;         // xlo xhi plo phi
 constexpr uint32_t kSlots = 2048;
 constexpr uint32_t kSlotWords = 9;          // xlo xhi q plo phi dlo dhi clo chi
 
 __host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) { return num_groups * kCubeDisc * kCubeWords * 4; }
+__host__ __device__ constexpr uint32_t cube3_bytes(uint32_t num_groups) {
+    return num_groups * kCubeDisc * kCubeTax * kCube3Words * 4;
+}
 __host__ __device__ constexpr uint32_t slot_bytes(uint32_t slots) { return slots * kSlotWords * 4; }
 
 // ---------------------------------------------------------------------------------------------
@@ -255,6 +263,74 @@ struct CubeTable {
                 CH += (unsigned __int128)(100u - d) * ((unsigned __int128)Pd * 100u + TPd);
 #pragma unroll
                 for (uint32_t k = 0; k < kCubeWords; ++k) w[k * cells + c] = 0;
+            }
+            if (cnt)
+                scratch_add(acc, g, cnt, q, dsum, P, (uint64_t)DP & 0xFFFFFFFFull, (uint64_t)(DP >> 32),
+                            (uint64_t)CH & 0xFFFFFFFFull, (uint64_t)(CH >> 32));
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Cube3Table: shared (group, discount, tax) cells, for num_groups <= 64. A row adds only its
+// count and quantity (one packed word) and its price: two atomics. At the flush the cell's
+// discount and tax give sum (100-d) p = (100-d) P and sum (100-d)(100+t) p = (100-d)(100+t) P.
+// ---------------------------------------------------------------------------------------------
+struct Cube3Table {
+    uint32_t* w;       // [kCube3Words][cells]
+    uint32_t cells;
+    __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
+        w = reinterpret_cast<uint32_t*>(base);
+        cells = num_groups * kCubeDisc * kCubeTax;
+    }
+    __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
+        for (uint32_t i = tid; i < kCube3Words * cells; i += nthreads) w[i] = 0;
+    }
+    __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
+                                             const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
+        uint32_t c[4], vx[4], ox[4], op[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            c[r] = (key[r] * kCubeDisc + d[r]) * kCubeTax + t[r];
+            vx[r] = 1u + (q[r] << 24);   // count + 2^24 * quantity
+            if ((m >> r) & 1u) {
+                ox[r] = atomicAdd(w + c[r], vx[r]);
+                op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if ((m >> r) & 1u) {
+                if (ox[r] + vx[r] < ox[r]) atomicAdd(w + cells + c[r], 1u);
+                if (op[r] + p[r] < op[r]) atomicAdd(w + 3 * cells + c[r], 1u);
+            }
+        }
+    }
+    // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
+    __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t tid, uint32_t nthreads) {
+        for (uint32_t g = tid; g < num_groups; g += nthreads) {
+            uint64_t cnt = 0, q = 0, dsum = 0, P = 0;
+            unsigned __int128 DP = 0, CH = 0;
+            for (uint32_t d = 0; d < kCubeDisc; ++d) {
+                uint64_t Pd = 0, cd = 0;
+                unsigned __int128 Td = 0;   // sum_t (100 + t) P_dt
+#pragma unroll
+                for (uint32_t t = 0; t < kCubeTax; ++t) {
+                    const uint32_t c = (g * kCubeDisc + d) * kCubeTax + t;
+                    const uint64_t X = ((uint64_t)w[cells + c] << 32) | w[c];
+                    const uint64_t Pt = ((uint64_t)w[3 * cells + c] << 32) | w[2 * cells + c];
+                    cd += X & 0xFFFFFFull;
+                    q += X >> 24;
+                    Pd += Pt;
+                    Td += (unsigned __int128)(100u + t) * Pt;
+#pragma unroll
+                    for (uint32_t k = 0; k < kCube3Words; ++k) w[k * cells + c] = 0;
+                }
+                cnt += cd;
+                dsum += (uint64_t)d * cd;
+                P += Pd;
+                DP += (unsigned __int128)(100u - d) * Pd;
+                CH += (unsigned __int128)(100u - d) * Td;
             }
             if (cnt)
                 scratch_add(acc, g, cnt, q, dsum, P, (uint64_t)DP & 0xFFFFFFFFull, (uint64_t)(DP >> 32),
