@@ -274,6 +274,8 @@ def main():
                          "launch vs one plain launch each; serve: Poisson request stream, served vs plain")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--groups", default="4,64,1024,65536", help="groupkey: group counts to sweep")
+    ap.add_argument("--batch-groups", default="4,64,1024", help="batch: group counts instances draw from")
+    ap.add_argument("--tune", type=int, default=1, help="batch: 0 heuristic placements, 1 autotuner")
     ap.add_argument("--ref-gpu", action="store_true",
                     help="with --impl reference: the reference's own GPU kernels on this GPU instead of its CPU kernels")
     ap.add_argument("--packing", default="pair", choices=["pair", "separate"],
@@ -552,12 +554,12 @@ def bench_groupkey(args):
 BATCH_BYTES_PER_ROW = 13      # ship 2 + qty 1 + disc 1 + tax 1 + price 4 + key 4
 
 
-def batch_instances(n, seed):
+def batch_instances(n, seed, group_choices=(4, 64, 1024)):
     import numpy as np
     rng = np.random.default_rng(seed)
     rows = np.exp(rng.uniform(np.log(1e4), np.log(5e7), n)).astype(np.int64)
     cutoffs = rng.integers(729906, 730090, n)
-    groups = rng.choice([4, 64, 1024], n)
+    groups = rng.choice(list(group_choices), n)
     return [(int(r), int(c), int(g)) for r, c, g in zip(rows, cutoffs, groups)]
 
 
@@ -572,7 +574,8 @@ def bench_batch(args):
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
     sh = ctypes.c_void_p(stream.cuda_stream)
-    spec = batch_instances(args.instances, SEED + 3)
+    choices = tuple(int(g) for g in args.batch_groups.split(","))
+    spec = batch_instances(args.instances, SEED + 3, choices)
     keep, descs, outs_b, outs_p, scratch = [], [], [], [], []
     for i, (rows, cutoff, g) in enumerate(spec):
         cols = {k: torch.empty(rows * w + 64, dtype=torch.uint8, device="cuda")
@@ -624,7 +627,7 @@ def bench_batch(args):
         cache = os.path.join(td, "tune.txt").encode()
         b = ctypes.c_void_p()
         t0 = time.perf_counter()
-        _lib.check(L.q1_batch_create(arr, len(descs), ctypes.byref(_lib.BatchOpts(1, 0, 0, 1, cache)), sh,
+        _lib.check(L.q1_batch_create(arr, len(descs), ctypes.byref(_lib.BatchOpts(1, 0, 0, args.tune, cache)), sh,
                                      ctypes.byref(b)))
         tune_s = time.perf_counter() - t0
         try:
@@ -655,7 +658,7 @@ def bench_batch(args):
             "dtype": "int64", "data": "synthetic",
             "config": {"workload": f"q1_batch_{len(spec)}_instances", "instances": len(spec), "total_rows": total_rows,
                        "rows": "log-uniform [1e4, 5e7]", "cutoff": "uniform [729906, 730089]",
-                       "groups": "{4, 64, 1024} uniform keys", "seed": SEED + 3,
+                       "groups": "{" + args.batch_groups.replace(",", ", ") + "} uniform keys", "seed": SEED + 3,
                        "l2": f"inputs {BATCH_BYTES_PER_ROW * total_rows / 1e9:.1f} GB per pass > 126 MB L2"},
             "batched": {"ms": ms_batch, "rows_per_s": total_rows / (ms_batch / 1e3), "gbs": gbs,
                         "frac_hbm": gbs / peak, "peak_kind": peak_kind, "items": desc.items, "grid": desc.grid,

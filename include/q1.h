@@ -417,6 +417,40 @@ q1_status q1_precompute_filter(const uint16_t* dev_shipdate, uint64_t rows, int3
                                uint32_t* dev_bitmap, void* cuda_stream);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Binary column cache: the reference's on-disk format (src/file_access.hpp:19-61, written and  */
+/* read by src/main.cu:405-474). A directory holds one raw native-endian array per column:     */
+/* shipdate.bin (int32 day numbers), returnflag.bin, linestatus.bin (char), discount.bin,       */
+/* tax.bin, extendedprice.bin, quantity.bin (int64 hundredths / cents).                          */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Writable reference-typed host columns (the output side of q1_columns). */
+typedef struct q1_columns_out {
+    int32_t* shipdate;
+    char*    returnflag;
+    char*    linestatus;
+    int64_t* discount;
+    int64_t* tax;
+    int64_t* extendedprice;
+    int64_t* quantity;
+} q1_columns_out;
+
+/* Writes `rows` rows of host columns as a cache directory (created if missing). */
+q1_status q1_cache_write(const char* dir, const q1_columns* host_columns, uint64_t rows);
+
+/* Rows of a cache directory: shipdate.bin's size / 4, every other file checked against it
+ * (Q1_ERR_INVALID_ARGUMENT on a missing or mis-sized file). Unlike src/main.cu:412-414, an
+ * SF-1-sized cache is never rescaled by a scale factor. */
+q1_status q1_cache_rows(const char* dir, uint64_t* rows);
+
+/* Reads a cache directory of exactly `rows` rows into caller-owned host columns. */
+q1_status q1_cache_read(const char* dir, uint64_t rows, q1_columns_out* out);
+
+/* Loads a cache directory into the context (compressing it when layout is COMPRESSED), like
+ * q1_load_columns; the row count is returned in rows_out (may be NULL). */
+q1_status q1_cache_load(q1_ctx* ctx, const char* dir, q1_layout layout, q1_flag_packing packing,
+                        q1_residency residency, uint64_t* rows_out);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Synthetic data generator (stands in for dbgen, scripts/genlineitem.sh)                       */
 /* ------------------------------------------------------------------------------------------ */
 

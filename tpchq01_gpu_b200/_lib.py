@@ -116,6 +116,11 @@ class BatchDesc(ctypes.Structure):
                 ("total_rows", ctypes.c_uint64), ("total_groups", ctypes.c_uint64)]
 
 
+class ColumnsOut(ctypes.Structure):
+    _fields_ = [("shipdate", vp), ("returnflag", vp), ("linestatus", vp), ("discount", vp), ("tax", vp),
+                ("extendedprice", vp), ("quantity", vp)]
+
+
 SERVE_MAX_GROUPS = 64
 SERVE_RESIDENT_KEY_GROUPS = 64
 REQ_RESIDENT, REQ_ADHOC = 0, 1
@@ -212,6 +217,11 @@ SIGNATURES = {
     "q1_server_resident_columns": (ctypes.c_int, [vp, ctypes.POINTER(CompressedColumns), ctypes.POINTER(vp),
                                                   ctypes.POINTER(ctypes.c_uint64)]),
     "q1_server_close": (ctypes.c_int, [vp]),
+    "q1_cache_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(Columns), ctypes.c_uint64]),
+    "q1_cache_rows": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "q1_cache_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ColumnsOut)]),
+    "q1_cache_load": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_uint64)]),
     "q1_version": (ctypes.c_char_p, []),
 }
 

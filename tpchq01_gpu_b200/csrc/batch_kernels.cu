@@ -134,7 +134,11 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
         // ------------------------------ consumers ---------------------------------------
         const uint32_t ctid = threadIdx.x;
         uint32_t cur = 0xFFFFFFFFu;
-        BatchInstanceDev in{};
+        // The instance's descriptor stays in global memory (read through the L1 when a flush or a
+        // partial tile needs it); only the fields of the row loop live in registers.
+        const BatchInstanceDev* in = nullptr;
+        uint32_t num_groups = 0;
+        int32_t cutoff = 0;
         uint32_t mode = kModeGlobal;
         uint32_t table = 0;   // 0 slots, 1 (group, discount) cube, 2 (group, discount, tax) cube
         uint32_t hot = 0;
@@ -159,32 +163,32 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
             rows_since = 0;
             if (cur == 0xFFFFFFFFu) return;
             if (mode == kModeRegisters) {
-                regs.flush(in.acc, in.num_groups, lane);
+                regs.flush(in->acc, num_groups, lane);
             } else if (mode == kModeShared) {
                 cb.sync(lane, prm.status);
-                if (table == 2) cube3.flush(in.acc, in.num_groups, ctid, W * 32);
-                else if (table == 1) cube.flush(in.acc, in.num_groups, ctid, W * 32);
-                else slots.flush(in.acc, ctid, W * 32);
+                if (table == 2) cube3.flush(in->acc, num_groups, ctid, W * 32);
+                else if (table == 1) cube.flush(in->acc, num_groups, ctid, W * 32);
+                else slots.flush(in->acc, ctid, W * 32);
                 cb.sync(lane, prm.status);
             }
         };
         auto add = [&](const ka::KeyQuad& x) {
             if (mode == kModeRegisters) {
-                regs.add(x, in.num_groups, bad);
+                regs.add(x, num_groups, bad);
             } else if (mode == kModeShared) {
-                if (table == 2) ka::table_quad(cube3, x, in.num_groups, hot, in.acc, bad);
-                else if (table == 1) ka::table_quad(cube, x, in.num_groups, hot, in.acc, bad);
-                else ka::table_quad(slots, x, in.num_groups, hot, in.acc, bad);
+                if (table == 2) ka::table_quad(cube3, x, num_groups, hot, in->acc, bad);
+                else if (table == 1) ka::table_quad(cube, x, num_groups, hot, in->acc, bad);
+                else ka::table_quad(slots, x, num_groups, hot, in->acc, bad);
             } else {
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
                     if (!((x.PM >> (8 * r)) & 1u)) continue;
                     const uint32_t key = x.k[r];
-                    if (key >= in.num_groups) {
+                    if (key >= num_groups) {
                         bad = 1u;
                         continue;
                     }
-                    ka::scratch_row(in.acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                    ka::scratch_row(in->acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
                                     (x.X >> (8 * r)) & 0xFFu, x.p[r]);
                 }
             }
@@ -200,13 +204,15 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
             if (m.instance != cur) {
                 flush();
                 cur = m.instance;
-                in = prm.inst[cur];
-                mode = in.mode;
-                if (mode == kModeRegisters && in.num_groups > 4) mode = kModeShared;   // planes hold 4 groups
-                table = in.num_groups <= ka::kCube3MaxGroups ? 2u : (in.num_groups <= ka::kCubeMaxGroups ? 1u : 0u);
-                hot = table ? in.num_groups : (in.num_groups < ka::kSlots ? in.num_groups : ka::kSlots);
-                if (table == 2) cube3.bind(tab, in.num_groups);
-                else if (table == 1) cube.bind(tab, in.num_groups);
+                in = prm.inst + cur;
+                mode = in->mode;
+                num_groups = in->num_groups;
+                cutoff = in->cutoff;
+                if (mode == kModeRegisters && num_groups > 4) mode = kModeShared;   // planes hold 4 groups
+                table = num_groups <= ka::kCube3MaxGroups ? 2u : (num_groups <= ka::kCubeMaxGroups ? 1u : 0u);
+                hot = table ? num_groups : (num_groups < ka::kSlots ? num_groups : ka::kSlots);
+                if (table == 2) cube3.bind(tab, num_groups);
+                else if (table == 1) cube.bind(tab, num_groups);
                 else slots.bind(tab, hot);
             } else if ((mode == kModeRegisters && tiles_since >= ka::kPlaneFlushTiles) ||
                        (mode == kModeShared && rows_since + m.rows > ka::kTableFlushRows)) {
@@ -215,12 +221,24 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
             ++tiles_since;
             rows_since += m.rows;
             if (m.kind == kKindFull) {
+                // one engine per tile: the mode test stays out of the row loop
                 const uint32_t base = ring + s * kStage;
+                if (mode == kModeRegisters) {
+#pragma unroll 1
+                    for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
+                        regs.add(ka::load_quad(base, ctid + itx * (W * 32), cutoff, bad), num_groups, bad);
+                } else if (mode == kModeShared && table == 2) {
 #pragma unroll
-                for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
-                    add(ka::load_quad(base, ctid + itx * (W * 32), in.cutoff, bad));
+                    for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
+                        ka::table_quad(cube3, ka::load_quad(base, ctid + itx * (W * 32), cutoff, bad), num_groups,
+                                       hot, in->acc, bad);
+                } else {
+#pragma unroll
+                    for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
+                        add(ka::load_quad(base, ctid + itx * (W * 32), cutoff, bad));
+                }
             } else {
-                for (uint32_t i = ctid; i < m.rows; i += W * 32) add(ka::load_row(in.col, m.row0 + i, in.cutoff, bad));
+                for (uint32_t i = ctid; i < m.rows; i += W * 32) add(ka::load_row(in->col, m.row0 + i, cutoff, bad));
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));

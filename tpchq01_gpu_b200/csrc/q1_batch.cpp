@@ -297,7 +297,8 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
         for (auto& kv : rep) {
             if (tune == 1 && modes.count(kv.first)) continue;
             const uint32_t i = kv.second;
-            if (!b->inst[i].rows) {
+            // Below 256 tiles a class's time is launch overhead, not placement: keep the heuristic.
+            if ((b->inst[i].rows + kBatchTileRows - 1) / kBatchTileRows < 256) {
                 modes[kv.first] = b->modes[i];
                 continue;
             }
@@ -305,8 +306,12 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
             if (b->inst[i].num_groups <= 4) cands.push_back(kModeRegisters);
             cands.push_back(kModeShared);
             cands.push_back(kModeGlobal);
-            uint32_t best = cands[0];
+            // the heuristic placement keeps the class unless another is faster by more than 3%
+            uint32_t best = saved_modes[i];
             float best_ms = 1e30f;
+            std::stable_sort(cands.begin(), cands.end(), [&](uint32_t a, uint32_t c) {
+                return (a == saved_modes[i]) > (c == saved_modes[i]);
+            });
             for (uint32_t m : cands) {
                 b->modes = saved_modes;
                 b->modes[i] = m;
@@ -318,6 +323,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
                 if ((st = upload(b.get())) != Q1_OK) return st;
                 float ms = 0;
                 if ((st = time_batch(b.get(), s, 3, &ms)) != Q1_OK) return st;
+                if (m != saved_modes[i]) ms *= 1.03f;
                 if (ms < best_ms) {
                     best_ms = ms;
                     best = m;

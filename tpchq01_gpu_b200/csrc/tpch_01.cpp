@@ -7,6 +7,8 @@
 // --tuples-per-thread= | --tuples_per_thread=, --tuples-per-kernel-launch= | --tuples-per-kernel=,
 // --runs=, --cpu-fraction=.
 // Additions: --rows=N (exact row count), --seed=S (generator seed), --cutoff-day=D,
+// --data-dir=DIR (the reference's column cache DIR/<scale factor>/*.bin), --cache-dir=DIR (a
+// cache directory itself), --write-cache (generate and write the cache when it is missing),
 // --resident (keep the table in HBM instead of streaming it from pinned host memory every run,
 // which is what the reference does).
 // The table comes from the seeded synthetic generator (dbgen's lineitem.tbl is not available);
@@ -15,6 +17,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <sys/stat.h>
+
 #include <fstream>
 #include <string>
 #include <vector>
@@ -33,6 +37,7 @@ static void print_help(const char* argv0) {
                     "      or in-registers, local-mem, per-thread-shared-mem)\n");
     fprintf(stderr, "   --runs=[default:5]\n");
     fprintf(stderr, "   --sf=[default:1.0] | --scale-factor=   --rows=N\n");
+    fprintf(stderr, "   --data-dir=DIR | --cache-dir=DIR   --write-cache\n");
     fprintf(stderr, "   --cpu-fraction=[default:0.5]\n");
     fprintf(stderr, "   --streams=[default:4]\n");
     fprintf(stderr, "   --threads-per-block=[multiple of 32]\n");
@@ -105,7 +110,8 @@ int main(int argc, char** argv) {
     double scale_factor = 1.0;
     uint64_t rows = 0;
     uint64_t seed = 20260101;
-    bool print = false, resident = false;
+    bool print = false, resident = false, write_cache = false;
+    std::string data_dir, cache_dir;
     for (int i = 1; i < argc; ++i) {
         std::string a(argv[i]);
         if (!starts(a, "--")) {
@@ -127,6 +133,9 @@ int main(int argc, char** argv) {
             else if (name == "use-filter-pushdown") p.use_filter_pushdown = 1;
             else if (name == "print-results") print = true;
             else if (name == "resident") resident = true;
+            else if (name == "data-dir") data_dir = val;
+            else if (name == "cache-dir") cache_dir = val;
+            else if (name == "write-cache") write_cache = true;
             else if (name == "scale-factor" || name == "sf") {
                 scale_factor = std::stod(val);
                 if (scale_factor < 0.001) {
@@ -171,18 +180,48 @@ int main(int argc, char** argv) {
         return EXIT_FAILURE;
     }
     const q1_residency res = resident ? Q1_RESIDENCY_HBM : Q1_RESIDENCY_PINNED_HOST;
-    printf("Generating %llu lineitem rows (seed %llu, %s, %s)... ", (unsigned long long)rows,
-           (unsigned long long)seed, p.apply_compression ? "compressed" : "uncompressed",
-           resident ? "HBM-resident" : "pinned host memory, streamed each run");
-    fflush(stdout);
-    q1_status st = q1_generate_table(ctx, seed, 0, rows, p.apply_compression ? Q1_LAYOUT_COMPRESSED : Q1_LAYOUT_UNCOMPRESSED,
-                                     Q1_FLAGS_PAIR_2BIT, res);
+    const q1_layout layout = p.apply_compression ? Q1_LAYOUT_COMPRESSED : Q1_LAYOUT_UNCOMPRESSED;
+    q1_status st;
+    if (!data_dir.empty() || !cache_dir.empty()) {
+        // the reference's column cache: <data dir>/<scale factor as std::to_string>/ (src/main.cu:405-409)
+        const std::string dir = !cache_dir.empty() ? cache_dir : data_dir + "/" + std::to_string(scale_factor);
+        uint64_t cached = 0;
+        if (q1_cache_rows(dir.c_str(), &cached) != Q1_OK) {
+            if (!write_cache) {
+                fprintf(stderr, "%s (use --write-cache to generate one)\n", q1_last_error());
+                q1_close(ctx);
+                return EXIT_FAILURE;
+            }
+            printf("Writing a column cache of %llu generated rows to %s... ", (unsigned long long)rows, dir.c_str());
+            fflush(stdout);
+            if (!data_dir.empty()) mkdir(data_dir.c_str(), 0755);
+            std::vector<int32_t> ship(rows);
+            std::vector<int64_t> disc(rows), price(rows), tax(rows), qty(rows);
+            std::vector<char> rf(rows), ls(rows);
+            q1_columns c{ship.data(), disc.data(), price.data(), tax.data(), qty.data(), rf.data(), ls.data()};
+            if (q1_generate_host(seed, 0, rows, &c) != Q1_OK || q1_cache_write(dir.c_str(), &c, rows) != Q1_OK) {
+                fprintf(stderr, "\n%s\n", q1_last_error());
+                q1_close(ctx);
+                return EXIT_FAILURE;
+            }
+            printf("done.\n");
+        }
+        printf("Loading the column cache in %s... ", dir.c_str());
+        fflush(stdout);
+        st = q1_cache_load(ctx, dir.c_str(), layout, Q1_FLAGS_PAIR_2BIT, res, &rows);
+    } else {
+        printf("Generating %llu lineitem rows (seed %llu, %s, %s)... ", (unsigned long long)rows,
+               (unsigned long long)seed, p.apply_compression ? "compressed" : "uncompressed",
+               resident ? "HBM-resident" : "pinned host memory, streamed each run");
+        fflush(stdout);
+        st = q1_generate_table(ctx, seed, 0, rows, layout, Q1_FLAGS_PAIR_2BIT, res);
+    }
     if (st != Q1_OK) {
-        fprintf(stderr, "\ntable generation failed: %s\n", q1_last_error());
+        fprintf(stderr, "\nloading the table failed: %s\n", q1_last_error());
         q1_close(ctx);
         return EXIT_FAILURE;
     }
-    printf("done.\n");
+    printf("done (%llu rows).\n", (unsigned long long)rows);
     std::ofstream csv("results.csv", std::ios::out);
     const int runs = p.runs;
     p.runs = 1;
