@@ -58,6 +58,129 @@ struct StageMeta {
 
 }  // namespace bk
 
+namespace bk {
+
+// The instance fields the row loop needs, kept in registers while an instance is current; the
+// descriptor itself stays in global memory (read through the L1 for flushes and partial tiles).
+struct Current {
+    const BatchInstanceDev* in;
+    uint32_t id;          // instance index, 0xFFFFFFFF before the first
+    uint32_t num_groups;
+    uint32_t hot;         // keys below `hot` go to the shared table
+    int32_t cutoff;
+};
+
+// Consumer side of one engine: processes stages until the producer's end-of-engine marker,
+// flushing the engine's accumulators whenever the instance changes and at the end. `k` is the
+// running stage counter shared by all engines of the CTA; returns false if a bounded wait
+// expired (the kernel then stops).
+template <int E>
+__device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t ring, uint8_t* tab, uint64_t* full_bar,
+                                               uint64_t* empty_bar, const StageMeta* meta, uint32_t& k,
+                                               ka::ConsumerBarrier& cb, uint32_t& bad) {
+    const uint32_t lane = threadIdx.x & 31u, ctid = threadIdx.x;
+    ka::PlaneRegs<4> regs;
+    ka::Cube3Table cube3;
+    ka::CubeTable cube;
+    ka::SlotTable slots;
+    if constexpr (E == kEngRegisters) regs.zero();
+    Current c{nullptr, 0xFFFFFFFFu, 0, 0, 0};
+    uint32_t tiles_since = 0;
+    uint64_t rows_since = 0;
+    bool ok = true;
+
+    auto flush = [&]() {
+        tiles_since = 0;
+        rows_since = 0;
+        if (c.id == 0xFFFFFFFFu) return;
+        if constexpr (E == kEngRegisters) {
+            regs.flush(c.in->acc, c.num_groups, lane);
+        } else if constexpr (E != kEngGlobal) {
+            cb.sync(lane, prm.status);
+            if constexpr (E == kEngCube3) cube3.flush(c.in->acc, c.num_groups, ctid, W * 32);
+            else if constexpr (E == kEngCube) cube.flush(c.in->acc, c.num_groups, ctid, W * 32);
+            else slots.flush(c.in->acc, ctid, W * 32);
+            cb.sync(lane, prm.status);
+        }
+    };
+    auto add = [&](const ka::KeyQuad& x) {
+        if constexpr (E == kEngRegisters) {
+            regs.add(x, c.num_groups, bad);
+        } else if constexpr (E == kEngCube3) {
+            ka::table_quad(cube3, x, c.num_groups, c.hot, c.in->acc, bad);
+        } else if constexpr (E == kEngCube) {
+            ka::table_quad(cube, x, c.num_groups, c.hot, c.in->acc, bad);
+        } else if constexpr (E == kEngSlots) {
+            ka::table_quad(slots, x, c.num_groups, c.hot, c.in->acc, bad);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (!((x.PM >> (8 * r)) & 1u)) continue;
+                const uint32_t key = x.k[r];
+                if (key >= c.num_groups) {
+                    bad = 1u;
+                    continue;
+                }
+                ka::scratch_row(c.in->acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                                (x.X >> (8 * r)) & 0xFFu, x.p[r]);
+            }
+        }
+    };
+
+    for (;; ++k) {
+        const uint32_t s = k % S;
+        const bool landed = mbar_wait(smem_addr(&full_bar[s]), (k / S) & 1u, prm.status);
+        if (!__all_sync(0xffffffffu, landed)) {
+            ok = false;
+            break;
+        }
+        const StageMeta m = meta[s];
+        if (m.kind == kKindEnd) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
+            ++k;
+            break;
+        }
+        if (m.instance != c.id) {
+            flush();
+            c.id = m.instance;
+            c.in = prm.inst + m.instance;
+            c.num_groups = c.in->num_groups;
+            c.cutoff = c.in->cutoff;
+            c.hot = (E == kEngSlots && c.num_groups > ka::kSlots) ? ka::kSlots : c.num_groups;
+            if constexpr (E == kEngCube3) cube3.bind(tab, c.num_groups);
+            if constexpr (E == kEngCube) cube.bind(tab, c.num_groups);
+            if constexpr (E == kEngSlots) slots.bind(tab, c.hot);
+        } else if ((E == kEngRegisters && tiles_since >= ka::kPlaneFlushTiles) ||
+                   (E != kEngRegisters && E != kEngGlobal && rows_since + m.rows > ka::kTableFlushRows)) {
+            flush();
+        }
+        ++tiles_since;
+        rows_since += m.rows;
+        if (m.kind == kKindFull) {
+            const uint32_t base = ring + s * kStage;
+#pragma unroll
+            for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
+                add(ka::load_quad(base, ctid + itx * (W * 32), c.cutoff, bad));
+        } else {
+            for (uint32_t i = ctid; i < m.rows; i += W * 32) add(ka::load_row(c.in->col, m.row0 + i, c.cutoff, bad));
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
+    }
+    flush();
+    return ok;
+}
+
+// Engine a CTA starts with: the role ranges of the grid, then every other engine in turn.
+__device__ __forceinline__ uint32_t first_engine(const BatchParams& prm) {
+    uint32_t e = 0;
+    while (e + 1 < kEngines && blockIdx.x >= prm.role_end[e]) ++e;
+    return e;
+}
+
+}  // namespace bk
+
 __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __grid_constant__ BatchParams prm) {
     using namespace bk;
     extern __shared__ __align__(128) uint8_t smem[];
@@ -69,6 +192,7 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t ring = smem_addr(smem);
     uint8_t* const tab = smem + S * kStage;   // shared table, all zero between instances
+    const uint32_t e0 = first_engine(prm);
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < S; ++s) {
@@ -83,171 +207,82 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
 
     if (warp == W) {
         // ------------------------------ producer ----------------------------------------
+        // Engines in the CTA's order; per engine, claim items from its queue until it is empty,
+        // stream their tiles, then post an end-of-engine marker.
         if (lane == 0) {
             const uint64_t pol = policy_evict_first();
             uint32_t k = 0;
             bool ok = true;
-            for (;;) {
-                const uint32_t item_idx = atomicAdd(prm.cursor, 1u);
-                if (item_idx >= prm.num_items) break;
-                const BatchItem it = prm.items[item_idx];
-                const BatchInstanceDev& in = prm.inst[it.instance];
-                for (uint32_t tt = 0; tt < it.num_tiles && ok; ++tt, ++k) {
-                    const uint32_t s = k % S;
-                    if (!mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) {
-                        ok = false;
-                        break;
-                    }
-                    const uint64_t tile = (uint64_t)it.first_tile + tt;
-                    const uint64_t row0 = tile * R;
-                    const uint32_t n = (uint32_t)(in.rows - row0 < R ? in.rows - row0 : R);
-                    meta[s].instance = it.instance;
-                    meta[s].row0 = row0;
-                    meta[s].rows = n;
-                    const uint32_t fb = smem_addr(&full_bar[s]);
-                    if (n == R) {
-                        meta[s].kind = kKindFull;
-                        mbar_arrive_expect_tx(fb, kStage);
+            for (uint32_t step = 0; step < kEngines && ok; ++step) {
+                const uint32_t e = (e0 + step) % kEngines;
+                const uint32_t count = prm.item_begin[e + 1] - prm.item_begin[e];
+                for (;;) {
+                    const uint32_t idx = count ? atomicAdd(prm.cursor + e, 1u) : count;
+                    if (idx >= count) break;
+                    const BatchItem it = prm.items[prm.item_begin[e] + idx];
+                    const BatchInstanceDev& in = prm.inst[it.instance];
+                    for (uint32_t tt = 0; tt < it.num_tiles && ok; ++tt, ++k) {
+                        const uint32_t s = k % S;
+                        if (!mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) {
+                            ok = false;
+                            break;
+                        }
+                        const uint64_t tile = (uint64_t)it.first_tile + tt;
+                        const uint64_t row0 = tile * R;
+                        const uint32_t n = (uint32_t)(in.rows - row0 < R ? in.rows - row0 : R);
+                        meta[s].instance = it.instance;
+                        meta[s].row0 = row0;
+                        meta[s].rows = n;
+                        const uint32_t fb = smem_addr(&full_bar[s]);
+                        if (n == R) {
+                            meta[s].kind = kKindFull;
+                            mbar_arrive_expect_tx(fb, kStage);
 #pragma unroll
-                        for (int c = 0; c < 6; ++c)
-                            bulk_g2s(ring + s * kStage + ka::col_off(c), in.col[c] + tile * (uint64_t)ka::col_bytes(c),
-                                     ka::col_bytes(c), fb, pol);
-                    } else {
-                        meta[s].kind = kKindPartial;
-                        mbar_arrive(fb);
+                            for (int c = 0; c < 6; ++c)
+                                bulk_g2s(ring + s * kStage + ka::col_off(c), in.col[c] + tile * (uint64_t)ka::col_bytes(c),
+                                         ka::col_bytes(c), fb, pol);
+                        } else {
+                            meta[s].kind = kKindPartial;
+                            mbar_arrive(fb);
+                        }
                     }
+                    if (!ok) break;
                 }
                 if (!ok) break;
-            }
-            // end marker for the consumers
-            if (ok) {
+                // end-of-engine marker
                 const uint32_t s = k % S;
-                if (mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) {
-                    meta[s].kind = kKindEnd;
-                    mbar_arrive(smem_addr(&full_bar[s]));
-                    ++k;
+                if (!mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) {
+                    ok = false;
+                    break;
                 }
+                meta[s].kind = kKindEnd;
+                mbar_arrive(smem_addr(&full_bar[s]));
+                ++k;
             }
             for (uint32_t i = (k > S ? k - S : 0u); i < k; ++i) mbar_wait(smem_addr(&full_bar[i % S]), (i / S) & 1u, prm.status);
         }
     } else {
         // ------------------------------ consumers ---------------------------------------
-        const uint32_t ctid = threadIdx.x;
-        uint32_t cur = 0xFFFFFFFFu;
-        // The instance's descriptor stays in global memory (read through the L1 when a flush or a
-        // partial tile needs it); only the fields of the row loop live in registers.
-        const BatchInstanceDev* in = nullptr;
-        uint32_t num_groups = 0;
-        int32_t cutoff = 0;
-        uint32_t mode = kModeGlobal;
-        uint32_t table = 0;   // 0 slots, 1 (group, discount) cube, 2 (group, discount, tax) cube
-        uint32_t hot = 0;
-        ka::PlaneRegs<4> regs;
-        regs.zero();
-        ka::Cube3Table cube3;
-        ka::CubeTable cube;
-        ka::SlotTable slots;
-        cube3.bind(tab, 0);
-        cube.bind(tab, 0);
-        slots.bind(tab, 0);
+        // The same engine order; each engine's loop keeps only its own accumulators live.
         ka::ConsumerBarrier cb{smem_addr(&consumers_bar), 0};
-        uint32_t bad = 0;
-        // Tiles / rows added since the last flush (the same in every consumer thread): plane
-        // partials are flushed every ka::kPlaneFlushTiles tiles, shared tables before they would
-        // exceed ka::kTableFlushRows rows, and both whenever the instance changes. A flush of a
-        // shared table leaves it all zero.
-        uint32_t tiles_since = 0;
-        uint64_t rows_since = 0;
-        auto flush = [&]() {
-            tiles_since = 0;
-            rows_since = 0;
-            if (cur == 0xFFFFFFFFu) return;
-            if (mode == kModeRegisters) {
-                regs.flush(in->acc, num_groups, lane);
-            } else if (mode == kModeShared) {
-                cb.sync(lane, prm.status);
-                if (table == 2) cube3.flush(in->acc, num_groups, ctid, W * 32);
-                else if (table == 1) cube.flush(in->acc, num_groups, ctid, W * 32);
-                else slots.flush(in->acc, ctid, W * 32);
-                cb.sync(lane, prm.status);
+        uint32_t bad = 0, k = 0;
+        for (uint32_t step = 0; step < kEngines; ++step) {
+            const uint32_t e = (e0 + step) % kEngines;
+            bool ok;
+            switch (e) {
+                case kEngRegisters: ok = consume_engine<kEngRegisters>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                case kEngCube3: ok = consume_engine<kEngCube3>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                case kEngCube: ok = consume_engine<kEngCube>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                case kEngSlots: ok = consume_engine<kEngSlots>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                default: ok = consume_engine<kEngGlobal>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
             }
-        };
-        auto add = [&](const ka::KeyQuad& x) {
-            if (mode == kModeRegisters) {
-                regs.add(x, num_groups, bad);
-            } else if (mode == kModeShared) {
-                if (table == 2) ka::table_quad(cube3, x, num_groups, hot, in->acc, bad);
-                else if (table == 1) ka::table_quad(cube, x, num_groups, hot, in->acc, bad);
-                else ka::table_quad(slots, x, num_groups, hot, in->acc, bad);
-            } else {
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    if (!((x.PM >> (8 * r)) & 1u)) continue;
-                    const uint32_t key = x.k[r];
-                    if (key >= num_groups) {
-                        bad = 1u;
-                        continue;
-                    }
-                    ka::scratch_row(in->acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
-                                    (x.X >> (8 * r)) & 0xFFu, x.p[r]);
-                }
-            }
-        };
-
-        uint32_t k = 0;
-        for (;; ++k) {
-            const uint32_t s = k % S;
-            const bool landed = mbar_wait(smem_addr(&full_bar[s]), (k / S) & 1u, prm.status);
-            if (!__all_sync(0xffffffffu, landed)) break;
-            const StageMeta m = meta[s];
-            if (m.kind == kKindEnd) break;
-            if (m.instance != cur) {
-                flush();
-                cur = m.instance;
-                in = prm.inst + cur;
-                mode = in->mode;
-                num_groups = in->num_groups;
-                cutoff = in->cutoff;
-                if (mode == kModeRegisters && num_groups > 4) mode = kModeShared;   // planes hold 4 groups
-                table = num_groups <= ka::kCube3MaxGroups ? 2u : (num_groups <= ka::kCubeMaxGroups ? 1u : 0u);
-                hot = table ? num_groups : (num_groups < ka::kSlots ? num_groups : ka::kSlots);
-                if (table == 2) cube3.bind(tab, num_groups);
-                else if (table == 1) cube.bind(tab, num_groups);
-                else slots.bind(tab, hot);
-            } else if ((mode == kModeRegisters && tiles_since >= ka::kPlaneFlushTiles) ||
-                       (mode == kModeShared && rows_since + m.rows > ka::kTableFlushRows)) {
-                flush();
-            }
-            ++tiles_since;
-            rows_since += m.rows;
-            if (m.kind == kKindFull) {
-                // one engine per tile: the mode test stays out of the row loop
-                const uint32_t base = ring + s * kStage;
-                if (mode == kModeRegisters) {
-#pragma unroll 1
-                    for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
-                        regs.add(ka::load_quad(base, ctid + itx * (W * 32), cutoff, bad), num_groups, bad);
-                } else if (mode == kModeShared && table == 2) {
-#pragma unroll
-                    for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
-                        ka::table_quad(cube3, ka::load_quad(base, ctid + itx * (W * 32), cutoff, bad), num_groups,
-                                       hot, in->acc, bad);
-                } else {
-#pragma unroll
-                    for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
-                        add(ka::load_quad(base, ctid + itx * (W * 32), cutoff, bad));
-                }
-            } else {
-                for (uint32_t i = ctid; i < m.rows; i += W * 32) add(ka::load_row(in->col, m.row0 + i, cutoff, bad));
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
+            if (!ok) break;
         }
-        flush();
         if (bad && prm.status) atomicOr(prm.status, kStatusDomain);
     }
     __syncthreads();
 }
+
 
 // scratch of every instance -> its int128 table (+=); one thread per (instance, group).
 __global__ void __launch_bounds__(256) q1_batch_finalize(const BatchInstanceDev* __restrict__ inst,

@@ -95,6 +95,81 @@ void save_cache(const std::string& path) {
 
 }  // namespace
 
+uint32_t q1::batch_engine(uint32_t mode, uint32_t num_groups) {
+    if (mode == kModeRegisters && num_groups <= 4) return kEngRegisters;
+    if (mode == kModeGlobal) return kEngGlobal;
+    if (num_groups <= 64) return kEngCube3;
+    if (num_groups <= 256) return kEngCube;
+    return kEngSlots;
+}
+
+namespace {
+
+// Relative cost of a row per engine (time per row of the group-key kernel on a B200, registers =
+// 1): used only to size each engine's share of the grid.
+constexpr double kEngineCost[kEngines] = {1.0, 2.0, 2.3, 3.1, 10.0};
+
+void plan_items(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, int only, std::vector<BatchItem>& items,
+                uint32_t begin[kEngines + 1]) {
+    std::vector<BatchItem> per[kEngines];
+    for (uint32_t i = 0; i < n; ++i) {
+        if (only >= 0 && i != (uint32_t)only) continue;
+        const uint32_t e = batch_engine(inst[i].mode, inst[i].num_groups);
+        const uint64_t tiles = (inst[i].rows + kBatchTileRows - 1) / kBatchTileRows;
+        for (uint64_t t = 0; t < tiles; t += chunk) {
+            BatchItem it{};
+            it.instance = i;
+            it.first_tile = (uint32_t)t;
+            it.num_tiles = (uint32_t)std::min<uint64_t>(chunk, tiles - t);
+            per[e].push_back(it);
+        }
+    }
+    items.clear();
+    for (uint32_t e = 0; e < kEngines; ++e) {
+        // largest items first: the atomic cursor then hands out an engine's work in LPT order
+        std::stable_sort(per[e].begin(), per[e].end(),
+                         [](const BatchItem& a, const BatchItem& c) { return a.num_tiles > c.num_tiles; });
+        begin[e] = (uint32_t)items.size();
+        items.insert(items.end(), per[e].begin(), per[e].end());
+    }
+    begin[kEngines] = (uint32_t)items.size();
+}
+
+// CTAs per engine in proportion to the engine's estimated cost (at least one for an engine with
+// work when the grid allows); returns the grid actually used.
+uint32_t plan_roles(const BatchInstanceDev* inst, const std::vector<BatchItem>& items, const uint32_t begin[kEngines + 1],
+                    uint32_t grid, uint32_t role_end[kEngines]) {
+    grid = std::max<uint32_t>(1, std::min<uint32_t>(grid, (uint32_t)items.size()));
+    double cost[kEngines] = {0, 0, 0, 0, 0}, total = 0;
+    for (uint32_t e = 0; e < kEngines; ++e) {
+        for (uint32_t j = begin[e]; j < begin[e + 1]; ++j) cost[e] += (double)items[j].num_tiles * kEngineCost[e];
+        total += cost[e];
+    }
+    uint32_t share[kEngines] = {0, 0, 0, 0, 0}, used = 0;
+    for (uint32_t e = 0; e < kEngines; ++e) {
+        if (cost[e] <= 0) continue;
+        share[e] = std::max<uint32_t>(1, (uint32_t)(grid * cost[e] / (total > 0 ? total : 1)));
+        used += share[e];
+    }
+    // trim or pad the largest share so the shares sum to the grid
+    uint32_t big = 0;
+    for (uint32_t e = 1; e < kEngines; ++e)
+        if (share[e] > share[big]) big = e;
+    if (used > grid) share[big] -= std::min(share[big] - 1, used - grid);
+    else share[big] += grid - used;
+    uint32_t acc = 0;
+    for (uint32_t e = 0; e < kEngines; ++e) role_end[e] = (acc += share[e]);
+    return grid;
+}
+
+}  // namespace
+
+void q1::batch_plan(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, uint32_t grid, std::vector<BatchItem>& items,
+                    BatchParams& prm) {
+    plan_items(inst, n, std::max<uint32_t>(1, chunk), -1, items, prm.item_begin);
+    plan_roles(inst, items, prm.item_begin, grid, prm.role_end);
+}
+
 struct q1_batch {
     int device = 0;
     DeviceInfo* di = nullptr;
@@ -104,6 +179,8 @@ struct q1_batch {
     std::vector<ClassKey> cls;
     std::vector<uint32_t> modes;
     std::vector<BatchItem> items;
+    BatchParams roles{};                     // item_begin / role_end of `items`
+    uint32_t launch_grid = 0;
     uint64_t total_groups = 0;
     uint64_t total_rows = 0;
     uint32_t chunk = 0;
@@ -117,21 +194,11 @@ struct q1_batch {
     uint32_t tuned_classes = 0;
 };
 
-static void build_items(q1_batch* b, uint32_t chunk, std::vector<BatchItem>* out) {
-    out->clear();
-    for (uint32_t i = 0; i < b->n; ++i) {
-        const uint64_t tiles = (b->inst[i].rows + kBatchTileRows - 1) / kBatchTileRows;
-        for (uint64_t t = 0; t < tiles; t += chunk) {
-            BatchItem it{};
-            it.instance = i;
-            it.first_tile = (uint32_t)t;
-            it.num_tiles = (uint32_t)std::min<uint64_t>(chunk, tiles - t);
-            out->push_back(it);
-        }
-    }
-    // largest items first: the atomic cursor then hands out work in LPT order
-    std::stable_sort(out->begin(), out->end(),
-                     [](const BatchItem& a, const BatchItem& c) { return a.num_tiles > c.num_tiles; });
+// Items of every instance (only < 0) or of one instance, grouped by engine, and the grid roles.
+static void build_items(q1_batch* b, uint32_t chunk, int only = -1) {
+    for (uint32_t i = 0; i < b->n; ++i) b->inst[i].mode = b->modes[i];
+    plan_items(b->inst.data(), b->n, std::max<uint32_t>(1, chunk), only, b->items, b->roles.item_begin);
+    b->launch_grid = plan_roles(b->inst.data(), b->items, b->roles.item_begin, b->grid, b->roles.role_end);
 }
 
 static q1_status upload(q1_batch* b) {
@@ -159,15 +226,14 @@ static q1_status enqueue(q1_batch* b, cudaStream_t s) {
                                           static_cast<const uint64_t*>(b->d_base.p), b->n, b->total_groups, s));
     }
     Q1_CUDA(cudaMemsetAsync(b->d_scratch.p, 0, b->total_groups * 64ull, s));
-    Q1_CUDA(cudaMemsetAsync(b->d_cursor.p, 0, 16, s));
+    Q1_CUDA(cudaMemsetAsync(b->d_cursor.p, 0, 4 * kEngines, s));
     if (!b->items.empty()) {
-        BatchParams prm{};
+        BatchParams prm = b->roles;
         prm.inst = static_cast<const BatchInstanceDev*>(b->d_inst.p);
         prm.items = static_cast<const BatchItem*>(b->d_items.p);
-        prm.num_items = (uint32_t)b->items.size();
         prm.cursor = static_cast<uint32_t*>(b->d_cursor.p);
         prm.status = b->di->status;
-        Q1_CUDA(launch_batch(prm, std::min<uint32_t>(b->grid, (uint32_t)b->items.size()), s));
+        Q1_CUDA(launch_batch(prm, b->launch_grid, s));
     }
     Q1_CUDA(launch_batch_finalize(static_cast<const BatchInstanceDev*>(b->d_inst.p),
                                   static_cast<const uint64_t*>(b->d_base.p), b->n, b->total_groups, s));
@@ -261,7 +327,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
     if ((st = b->d_inst.alloc(sizeof(BatchInstanceDev) * std::max<uint32_t>(1, n))) != Q1_OK) return st;
     if ((st = b->d_base.alloc(sizeof(uint64_t) * (n + 1))) != Q1_OK) return st;
     if ((st = b->d_scratch.alloc(b->total_groups * 64ull)) != Q1_OK) return st;
-    if ((st = b->d_cursor.alloc(16)) != Q1_OK) return st;
+    if ((st = b->d_cursor.alloc(4 * kEngines)) != Q1_OK) return st;
     unsigned long long* scratch = static_cast<unsigned long long*>(b->d_scratch.p);
     for (uint32_t i = 0; i < n; ++i) b->inst[i].acc = scratch + 8ull * b->group_base[i];
     Q1_CUDA(cudaMemcpy(b->d_base.p, b->group_base.data(), sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice));
@@ -317,9 +383,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
                 b->modes[i] = m;
                 const uint64_t tiles = (b->inst[i].rows + kBatchTileRows - 1) / kBatchTileRows;
                 const uint32_t c = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(1024, tiles / (b->grid * 4ull) + 1));
-                b->items.clear();
-                for (uint64_t t = 0; t < tiles; t += c)
-                    b->items.push_back(BatchItem{i, (uint32_t)t, (uint32_t)std::min<uint64_t>(c, tiles - t), 0});
+                build_items(b.get(), c, (int)i);
                 if ((st = upload(b.get())) != Q1_OK) return st;
                 float ms = 0;
                 if ((st = time_batch(b.get(), s, 3, &ms)) != Q1_OK) return st;
@@ -346,7 +410,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
                 std::vector<uint32_t> cands = {std::max<uint32_t>(2, base / 4), base, std::min<uint32_t>(4096, base * 4)};
                 float best_ms = 1e30f;
                 for (uint32_t c : cands) {
-                    build_items(b.get(), c, &b->items);
+                    build_items(b.get(), c);
                     if ((st = upload(b.get())) != Q1_OK) return st;
                     float ms = 0;
                     if ((st = time_batch(b.get(), s, 2, &ms)) != Q1_OK) return st;
@@ -360,7 +424,7 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
         }
         save_cache(b->cache);
     }
-    build_items(b.get(), b->chunk, &b->items);
+    build_items(b.get(), b->chunk);
     if ((st = upload(b.get())) != Q1_OK) return st;
     *out = b.release();
     return Q1_OK;
@@ -400,7 +464,7 @@ q1_status q1_batch_describe(q1_batch* b, q1_batch_desc* d) {
     d->items = (uint32_t)b->items.size();
     d->chunk_tiles = b->chunk;
     d->tile_rows = kBatchTileRows;
-    d->grid = b->grid;
+    d->grid = b->launch_grid;
     d->total_rows = b->total_rows;
     d->total_groups = b->total_groups;
     d->uses_graph = b->use_graph ? 1 : 0;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace q1 {
 
 constexpr uint32_t kBatchTileRows = 2048;
@@ -34,13 +36,31 @@ struct BatchItem {
     uint32_t pad;
 };
 
+// Engine that aggregates an instance inside the batch kernel (q1_keyagg.cuh).
+enum BatchEngine : uint32_t {
+    kEngRegisters = 0,   // PlaneRegs<4>
+    kEngCube3 = 1,       // (group, discount, tax) cells, <= 64 groups
+    kEngCube = 2,        // (group, discount) cells, <= 256 groups
+    kEngSlots = 3,       // slots for keys < 2048, larger keys spilled
+    kEngGlobal = 4,      // straight into scratch
+    kEngines = 5,
+};
+uint32_t batch_engine(uint32_t mode, uint32_t num_groups);
+
 struct BatchParams {
     const BatchInstanceDev* inst;
-    const BatchItem* items;
-    uint32_t num_items;
-    uint32_t* cursor;             // work-queue head, zeroed before every launch
+    const BatchItem* items;             // grouped by engine: [item_begin[e], item_begin[e + 1])
+    uint32_t item_begin[kEngines + 1];
+    uint32_t role_end[kEngines];        // CTAs [role_end[e-1], role_end[e]) start with engine e
+    uint32_t* cursor;                   // kEngines claim counters, zeroed before every launch
     uint32_t* status;
 };
+
+// Cuts every instance (host descriptors) into items of at most `chunk` tiles, groups them by
+// engine (largest first inside an engine) and gives each engine a share of the `grid` CTAs in
+// proportion to its estimated cost; fills prm.item_begin and prm.role_end.
+void batch_plan(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, uint32_t grid, std::vector<BatchItem>& items,
+                BatchParams& prm);
 
 uint32_t batch_smem_bytes();
 cudaError_t batch_prepare_launch();

@@ -468,16 +468,11 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
         ++ninst;
     }
     if (ninst) {
-        // work items: chunks of tiles, largest first
+        // work items: chunks of tiles grouped by engine, largest first; grid roles by engine cost
         const uint64_t chunk = std::max<uint64_t>(4, std::min<uint64_t>(1024, tiles / ((uint64_t)s->di->sm_count * 4)));
         std::vector<BatchItem> items;
-        for (uint32_t i = 0; i < ninst; ++i) {
-            const uint64_t t_i = (inst[i].rows + kBatchTileRows - 1) / kBatchTileRows;
-            for (uint64_t t = 0; t < t_i; t += chunk)
-                items.push_back(BatchItem{i, (uint32_t)t, (uint32_t)std::min<uint64_t>(chunk, t_i - t), 0});
-        }
-        std::stable_sort(items.begin(), items.end(),
-                         [](const BatchItem& a, const BatchItem& b) { return a.num_tiles > b.num_tiles; });
+        BatchParams prm{};
+        batch_plan(inst, ninst, (uint32_t)chunk, (uint32_t)s->di->sm_count, items, prm);
         if ((r = grow_items(s, items.size())) != Q1_OK) return r;
         if (!items.empty()) {
             memcpy(s->h_items.p, items.data(), sizeof(BatchItem) * items.size());
@@ -487,14 +482,13 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
         Q1_CUDA(cudaMemcpyAsync(s->d_base.p, base, sizeof(uint64_t) * (ninst + 1), cudaMemcpyHostToDevice, st));
         Q1_CUDA(cudaMemsetAsync(s->d_scratch.p, 0, groups * 64, st));
         if (!items.empty()) {
-            Q1_CUDA(cudaMemsetAsync(s->d_cursor.p, 0, 16, st));
-            BatchParams prm{};
+            Q1_CUDA(cudaMemsetAsync(s->d_cursor.p, 0, 4 * kEngines, st));
             prm.inst = s->d_inst.as<BatchInstanceDev>();
             prm.items = s->d_items.as<BatchItem>();
-            prm.num_items = (uint32_t)items.size();
             prm.cursor = s->d_cursor.as<uint32_t>();
             prm.status = s->di->status;
-            Q1_CUDA(launch_batch(prm, (uint32_t)std::min<uint64_t>((uint64_t)s->di->sm_count, items.size()), st));
+            const uint32_t grid = prm.role_end[kEngines - 1];
+            Q1_CUDA(launch_batch(prm, grid, st));
         }
         Q1_CUDA(launch_batch_finalize(s->d_inst.as<BatchInstanceDev>(), s->d_base.as<uint64_t>(), ninst, groups, st));
     }
@@ -667,7 +661,7 @@ q1_status q1_server_open(const q1_server_opts* opts, q1_server** out) {
     if ((st = s->d_base.alloc(sizeof(uint64_t) * (m + 1))) != Q1_OK) return st;
     if ((st = s->h_base.alloc(sizeof(uint64_t) * (m + 1))) != Q1_OK) return st;
     if ((st = s->d_scratch.alloc(m * kMaxGroups * 64)) != Q1_OK) return st;
-    if ((st = s->d_cursor.alloc(16)) != Q1_OK) return st;
+    if ((st = s->d_cursor.alloc(4 * kEngines)) != Q1_OK) return st;
     if ((st = s->d_lookup.alloc(sizeof(CubeLookup) * m)) != Q1_OK) return st;
     if ((st = s->h_lookup.alloc(sizeof(CubeLookup) * m)) != Q1_OK) return st;
     if ((st = grow_items(s.get(), 4096)) != Q1_OK) return st;
