@@ -163,7 +163,11 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
             for (uint32_t itx = 0; itx < kSteps / (W * 32); ++itx)
                 add(ka::load_quad(base, ctid + itx * (W * 32), c.cutoff, bad));
         } else {
-            for (uint32_t i = ctid; i < m.rows; i += W * 32) add(ka::load_row(c.in->col, m.row0 + i, c.cutoff, bad));
+            // every lane runs every round (the table engines vote across the warp)
+            for (uint32_t i0 = 0; i0 < m.rows; i0 += W * 32) {
+                const uint32_t i = i0 + ctid;
+                add(i < m.rows ? ka::load_row(c.in->col, m.row0 + i, c.cutoff, bad) : ka::empty_quad());
+            }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));

@@ -194,8 +194,11 @@ __global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const 
         // the rows after the last full tile, by one CTA straight from global memory
         if (ok && blockIdx.x == (uint32_t)(num_tiles % gridDim.x) && num_tiles * R < prm.rows) {
             if (P == kPlaceSharedMemPerThread && rows_since + R > ka::kTableFlushRows) table_flush();
-            for (uint64_t i = num_tiles * R + ctid; i < prm.rows; i += W * 32)
-                add_quad(ka::load_row(prm.col, i, prm.cutoff, bad));
+            // every lane runs every round (the table engines vote across the warp)
+            for (uint64_t i0 = num_tiles * R; i0 < prm.rows; i0 += W * 32) {
+                const uint64_t i = i0 + ctid;
+                add_quad(i < prm.rows ? ka::load_row(prm.col, i, prm.cutoff, bad) : ka::empty_quad());
+            }
         }
         if (bad && prm.status) atomicOr(prm.status, kStatusDomain);
         if (P == kPlaceInRegistersPerThread) regs.flush(prm.acc, G, lane);

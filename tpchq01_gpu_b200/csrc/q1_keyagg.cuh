@@ -141,6 +141,16 @@ __device__ __forceinline__ KeyQuad load_quad(uint32_t base, uint32_t j, int32_t 
     return x;
 }
 
+// A quad with no passing row (for lanes past the end of a partial tile, so that every lane of
+// the warp takes part in the warp votes of the table engines).
+__device__ __forceinline__ KeyQuad empty_quad() {
+    KeyQuad x;
+    x.PM = x.Q = x.D = x.X = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) x.p[r] = x.k[r] = 0;
+    return x;
+}
+
 // One row read from global memory (tail rows of a partial tile), as a quad whose rows 1..3 fail.
 __device__ __forceinline__ KeyQuad load_row(const uint8_t* const col[6], uint64_t i, int32_t cut, uint32_t& bad) {
     KeyQuad x;
@@ -222,12 +232,13 @@ struct CubeTable {
     // atomics of the quad are issued before any carry is checked, so their latencies overlap.
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
-        uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4];
+        uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4], carry = 0;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             c[r] = key[r] * kCubeDisc + d[r];
             vx[r] = 1u + (q[r] << 24);   // count + 2^24 * quantity
             vt[r] = t[r] * p[r];         // < 2^28
+            ox[r] = op[r] = ot[r] = 0;
             if ((m >> r) & 1u) {
                 ox[r] = atomicAdd(w + c[r], vx[r]);
                 op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
@@ -236,10 +247,17 @@ struct CubeTable {
         }
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            if ((m >> r) & 1u) {
-                if (ox[r] + vx[r] < ox[r]) atomicAdd(w + cells + c[r], 1u);
-                if (op[r] + p[r] < op[r]) atomicAdd(w + 3 * cells + c[r], 1u);
-                if (ot[r] + vt[r] < ot[r]) atomicAdd(w + 5 * cells + c[r], 1u);
+            const uint32_t on = (m >> r) & 1u;
+            carry |= (on & (ox[r] + vx[r] < ox[r] ? 1u : 0u)) << (3 * r);
+            carry |= (on & (op[r] + p[r] < op[r] ? 1u : 0u)) << (3 * r + 1);
+            carry |= (on & (ot[r] + vt[r] < ot[r] ? 1u : 0u)) << (3 * r + 2);
+        }
+        if (__any_sync(0xffffffffu, carry)) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if ((carry >> (3 * r)) & 1u) atomicAdd(w + cells + c[r], 1u);
+                if ((carry >> (3 * r + 1)) & 1u) atomicAdd(w + 3 * cells + c[r], 1u);
+                if ((carry >> (3 * r + 2)) & 1u) atomicAdd(w + 5 * cells + c[r], 1u);
             }
         }
     }
@@ -288,11 +306,12 @@ struct Cube3Table {
     }
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
-        uint32_t c[4], vx[4], ox[4], op[4];
+        uint32_t c[4], vx[4], ox[4], op[4], carry = 0;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             c[r] = (key[r] * kCubeDisc + d[r]) * kCubeTax + t[r];
             vx[r] = 1u + (q[r] << 24);   // count + 2^24 * quantity
+            ox[r] = op[r] = 0;
             if ((m >> r) & 1u) {
                 ox[r] = atomicAdd(w + c[r], vx[r]);
                 op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
@@ -300,9 +319,16 @@ struct Cube3Table {
         }
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            if ((m >> r) & 1u) {
-                if (ox[r] + vx[r] < ox[r]) atomicAdd(w + cells + c[r], 1u);
-                if (op[r] + p[r] < op[r]) atomicAdd(w + 3 * cells + c[r], 1u);
+            const uint32_t on = (m >> r) & 1u;
+            carry |= (on & (ox[r] + vx[r] < ox[r] ? 1u : 0u)) << (2 * r);
+            carry |= (on & (op[r] + p[r] < op[r] ? 1u : 0u)) << (2 * r + 1);
+        }
+        // words wrap rarely (the price word every few hundred rows of a cell): one vote
+        if (__any_sync(0xffffffffu, carry)) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if ((carry >> (2 * r)) & 1u) atomicAdd(w + cells + c[r], 1u);
+                if ((carry >> (2 * r + 1)) & 1u) atomicAdd(w + 3 * cells + c[r], 1u);
             }
         }
     }
@@ -357,7 +383,7 @@ struct SlotTable {
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
         const uint32_t S = slots;
-        uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4];
+        uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4], carry = 0;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const uint32_t a = 100u - d[r];
@@ -366,10 +392,11 @@ struct SlotTable {
             const uint64_t c64 = (uint64_t)(a * (100u + t[r])) * p[r];
             cl[r] = (uint32_t)c64;
             ch[r] = (uint32_t)(c64 >> 32);
+            ox[r] = op[r] = od[r] = oc[r] = 0;
             if ((m >> r) & 1u) {
                 const uint32_t s = key[r];
                 ox[r] = atomicAdd(w + s, vx[r]);
-                if (q[r]) atomicAdd(w + 2 * S + s, q[r]);
+                atomicAdd(w + 2 * S + s, q[r]);
                 op[r] = atomicAdd(w + 3 * S + s, p[r]);
                 od[r] = atomicAdd(w + 5 * S + s, vd[r]);
                 oc[r] = atomicAdd(w + 7 * S + s, cl[r]);
@@ -377,13 +404,22 @@ struct SlotTable {
         }
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            if ((m >> r) & 1u) {
-                const uint32_t s = key[r];
-                if (ox[r] + vx[r] < ox[r]) atomicAdd(w + S + s, 1u);
-                if (op[r] + p[r] < op[r]) atomicAdd(w + 4 * S + s, 1u);
-                if (od[r] + vd[r] < od[r]) atomicAdd(w + 6 * S + s, 1u);
-                const uint32_t h = ch[r] + (oc[r] + cl[r] < oc[r] ? 1u : 0u);
-                if (h) atomicAdd(w + 8 * S + s, h);
+            const uint32_t on = (m >> r) & 1u;
+            carry |= (on & (ox[r] + vx[r] < ox[r] ? 1u : 0u)) << (3 * r);
+            carry |= (on & (op[r] + p[r] < op[r] ? 1u : 0u)) << (3 * r + 1);
+            carry |= (on & (od[r] + vd[r] < od[r] ? 1u : 0u)) << (3 * r + 2);
+            ch[r] = on ? ch[r] + (oc[r] + cl[r] < oc[r] ? 1u : 0u) : 0u;
+        }
+        // the charge's high word is nonzero for most rows: added per row
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (ch[r]) atomicAdd(w + 8 * S + key[r], ch[r]);
+        if (__any_sync(0xffffffffu, carry)) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if ((carry >> (3 * r)) & 1u) atomicAdd(w + S + key[r], 1u);
+                if ((carry >> (3 * r + 1)) & 1u) atomicAdd(w + 4 * S + key[r], 1u);
+                if ((carry >> (3 * r + 2)) & 1u) atomicAdd(w + 6 * S + key[r], 1u);
             }
         }
     }
@@ -406,24 +442,31 @@ struct SlotTable {
 // One quad into a shared table (CubeTable or SlotTable): rows in the table's fast domain go to the
 // table, other passing rows with key < num_groups straight to the scratch, passing rows with
 // key >= num_groups make `bad` nonzero.
+// All lanes of the warp call it (the slow path and the carries use warp votes).
 template <class Table>
 __device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_t num_groups, uint32_t hot,
                                            unsigned long long* acc, uint32_t& bad) {
-    uint32_t q[4], d[4], t[4], m = 0;
+    uint32_t q[4], d[4], t[4], m = 0, slow = 0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         q[r] = (x.Q >> (8 * r)) & 0xFFu;
         d[r] = (x.D >> (8 * r)) & 0xFFu;
         t[r] = (x.X >> (8 * r)) & 0xFFu;
-        const bool pass = (x.PM >> (8 * r)) & 1u;
+        const uint32_t pass = (x.PM >> (8 * r)) & 1u;
         const uint32_t key = x.k[r];
-        if (pass && key >= num_groups) bad = 1u;
-        if (pass && key < num_groups) {
-            if (key < hot && fast_domain(d[r], t[r], x.p[r])) m |= 1u << r;
-            else scratch_row(acc, key, q[r], d[r], t[r], x.p[r]);
-        }
+        const uint32_t in = pass & (key < num_groups ? 1u : 0u);
+        bad |= pass & (key >= num_groups ? 1u : 0u);
+        const uint32_t fast = in & (key < hot ? 1u : 0u) & (fast_domain(d[r], t[r], x.p[r]) ? 1u : 0u);
+        m |= fast << r;
+        slow |= (in & (fast ^ 1u)) << r;
     }
-    if (m) tab.add_quad(m, x.k, q, d, t, x.p);
+    // rows outside the tables' fast domain (none in TPC-H data): one vote skips the path
+    if (__any_sync(0xffffffffu, slow)) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if ((slow >> r) & 1u) scratch_row(acc, x.k[r], q[r], d[r], t[r], x.p[r]);
+    }
+    tab.add_quad(m, x.k, q, d, t, x.p);
 }
 
 // Barrier of the consumer warps only (the producer keeps streaming): one arrive per warp on an
