@@ -269,7 +269,7 @@ def main():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="scan", choices=["scan", "groupkey", "batch", "serve"],
+    ap.add_argument("--mode", default="scan", choices=["scan", "c1sweep", "groupkey", "batch", "serve"],
                     help="scan: the 600M-row aggregation (default); batch: 256 instances in one persistent "
                          "launch vs one plain launch each; serve: Poisson request stream, served vs plain")
     ap.add_argument("--instances", type=int, default=256)
@@ -286,6 +286,8 @@ def main():
     ROWS = args.rows
     if args.mode == "groupkey" and args.impl == "ours":
         return bench_groupkey(args)
+    if args.mode == "c1sweep" and args.impl == "ours":
+        return bench_c1sweep(args)
     if args.mode == "batch" and args.impl == "ours":
         return bench_batch(args)
     if args.mode == "serve" and args.impl == "ours":
@@ -449,6 +451,113 @@ def e2e_pinned(q, args):
                 "cpu_fraction": best, "cpu_fraction_sweep_ms": {str(k): 1000 * v for k, v in sweep.items()}}
     finally:
         ctx.close()
+
+
+# ------------------------------------------------------------------------------------------
+# --mode c1sweep: the 600M-row table in every HBM layout (pair / separate flags, filter pushdown
+# off / on, uncompressed) under every placement, then the host-streamed mode (pinned table) with
+# CPU fractions 0, 0.1, 0.25, 0.5, pushdown off / on. Every result is checked against the first.
+# ------------------------------------------------------------------------------------------
+
+def bench_c1sweep(args):
+    import ctypes
+    import torch
+    import tpchq01_gpu_b200 as q
+    from tpchq01_gpu_b200 import _lib
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    peak, _ = measured_peaks()
+    placements = ["in_registers_per_thread", "in_registers", "shared_mem_per_thread", "local_mem", "global"]
+    out = torch.zeros(72, dtype=torch.int64, device="cuda")
+    points, ref = [], None
+    reps = max(3, min(args.steps, 10))
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        q.sync_check(sh)
+        return a.elapsed_time(b) / reps
+
+    def record(layout, pushdown, placement, bpr, ms):
+        nonlocal ref
+        got = out.clone()
+        same = True if ref is None else bool(torch.equal(got, ref))
+        ref = got if ref is None else ref
+        gbs = bpr * ROWS / (ms / 1e3) / 1e9
+        points.append({"layout": layout, "pushdown": pushdown, "placement": placement, "ms": ms,
+                       "rows_per_s": ROWS / (ms / 1e3), "gbs": gbs, "frac_hbm": gbs / peak, "identical": same})
+        print(json.dumps(points[-1]), file=sys.stderr, flush=True)
+
+    for packing, bpr0 in [("pair", 9.25), ("separate", 9.375)]:
+        ctx = q.Q1Context()
+        ctx.generate(SEED, ROWS, layout="compressed", packing=packing)
+        comp, _, rows, _, _ = ctx.table_columns()
+        filt = torch.empty((rows + 31) // 32 + 8, dtype=torch.int32, device="cuda")
+        q.precompute_filter(comp.shipdate, rows, CUTOFF, filt.data_ptr(), sh)
+        comp.filter = filt.data_ptr()
+        for pushdown in [False, True]:
+            for pl in placements:
+                def fn():
+                    out.zero_()
+                    q.launch_compressed(pl, comp, rows, CUTOFF, pushdown, out.data_ptr(), sh)
+                ms = timed(fn)
+                record(packing, pushdown, pl, bpr0 - (1.875 if pushdown else 0.0), ms)
+        ctx.close()
+    # uncompressed: 100M rows (3.8 GB; the host generator stages the table in host memory)
+    ctx = q.Q1Context()
+    urows = min(ROWS, 100_000_000)
+    ctx.generate(SEED, urows, layout="uncompressed")
+    _, unc, rows, _, _ = ctx.table_columns()
+    uref = None
+    for pl in placements:
+        def fn():
+            out.zero_()
+            q.launch_uncompressed(pl, unc, rows, CUTOFF, out.data_ptr(), sh)
+        ms = timed(fn)
+        got = out.clone()
+        same = True if uref is None else bool(torch.equal(got, uref))
+        uref = got if uref is None else uref
+        gbs = 38.0 * rows / (ms / 1e3) / 1e9
+        points.append({"layout": "uncompressed", "rows": rows, "pushdown": False, "placement": pl, "ms": ms,
+                       "rows_per_s": rows / (ms / 1e3), "gbs": gbs, "frac_hbm": gbs / peak, "identical": same})
+        print(json.dumps(points[-1]), file=sys.stderr, flush=True)
+    ctx.close()
+
+    # host-streamed (pinned table, H2D inside every run)
+    streamed = []
+    ctx = q.Q1Context(cpu_threads=max(1, (os.cpu_count() or 2) - 2))
+    ctx.generate(SEED, ROWS, layout="compressed", packing="pair", residency="pinned")
+    for pushdown in [False, True]:
+        for frac in [0.0, 0.1, 0.25, 0.5]:
+            p = q.Q1Params(apply_compression=True, use_filter_pushdown=pushdown, use_coprocessing=frac > 0,
+                           cpu_processing_fraction=frac, num_gpu_streams=4, num_tuples_per_kernel_launch=1 << 24,
+                           num_query_execution_runs=1, cutoff_day=CUTOFF)
+            ctx.run(p)
+            t = []
+            for _ in range(3):
+                s0 = time.perf_counter()
+                ctx.run(p)
+                t.append(time.perf_counter() - s0)
+            ms = 1000 * min(t)
+            gpu_b = ROWS * (1 - frac) * (7.375 if pushdown else 9.25)
+            streamed.append({"pushdown": pushdown, "cpu_fraction": frac, "ms": ms, "rows_per_s": ROWS / (ms / 1e3),
+                             "pcie_gbs": gpu_b / (ms / 1e3) / 1e9})
+            print(json.dumps(streamed[-1]), file=sys.stderr, flush=True)
+    ctx.close()
+    line = {"metric": METRIC, "mode": "c1sweep", "unit": UNIT, "n_gpus": 1, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + "_sweep", "rows": ROWS, "cutoff_day": CUTOFF},
+            "value": max(p_["rows_per_s"] for p_ in points), "higher_is_better": True,
+            "identical": all(p_["identical"] for p_ in points), "hbm": points, "host_streamed": streamed}
+    print(json.dumps(line), flush=True)
+    return 0 if line["identical"] else 1
 
 
 # ------------------------------------------------------------------------------------------

@@ -63,6 +63,38 @@ def test_launch_compressed(cuda, placement, packing, use_filter):
 
 
 @pytest.mark.parametrize("placement", PLACEMENTS)
+@pytest.mark.parametrize("packing", ["pair", "sep"])
+@pytest.mark.parametrize("frac", [0.0005, 0.3])
+def test_all_six_flag_groups(cuda, placement, packing, frac):
+    """Rows of the groups A/O and R/O (absent from TPC-H data) change some rows' line status to O:
+    every placement must still sum all six (returnflag, linestatus) groups exactly."""
+    cols = gen_np.generate(32, 0, 200_003)
+    rng = np.random.default_rng(int(frac * 1e4))
+    rf = cols["returnflag"].view(np.uint8)
+    ls = cols["linestatus"].view(np.uint8).copy()
+    idx = np.flatnonzero(rf != ord("N"))
+    pick = rng.choice(idx, max(1, int(frac * len(idx))), replace=False)
+    ls[pick] = ord("O")
+    cols["linestatus"] = ls.view("S1")
+    if packing == "pair":
+        # the pair dictionary holds at most 4 combinations: keep A/F, N/F, N/O, A/O (drop R rows)
+        keep = cols["returnflag"].view(np.uint8) != ord("R")
+        cols = {k: v[keep] for k, v in cols.items()}
+    comp = gen_np.compress(cols, packing)
+    cutoff = 729999
+    c, keep_ = device_compressed(comp)
+    buf = aggs_buffer()
+    stream = torch.cuda.current_stream().cuda_stream
+    q.launch_compressed(placement, c, len(cols["shipdate"]), cutoff, False, buf.data_ptr(), stream)
+    q.sync_check(stream)
+    want, flag = O.q1_compressed(comp, cutoff)
+    assert flag == 0
+    assert np.array_equal(read(buf), want)
+    g = read(buf)
+    assert g[1][0] > 0   # A/O rows counted
+
+
+@pytest.mark.parametrize("placement", PLACEMENTS)
 def test_launch_uncompressed_accumulates_like_reference(cuda, placement):
     cols = gen_np.generate(32, 0, 54_321)
     keep = {k: dev(v) for k, v in cols.items()}

@@ -238,13 +238,28 @@ struct AccPerThread {
             x.P[3] = p >> 24;
             x.ABL = ab & 0xFFu;
             x.ABH = ab >> 8;
-            add_quad(x);
+#pragma unroll
+            for (int i = 0; i < G; ++i) gq[i].add_quad(x.OH, (uint32_t)i, x);   // no warp vote: lanes diverge here
         }
     }
+    // Called by all lanes of the warp. With the six (returnflag, linestatus) groups of the separate
+    // flag layout, A/O and R/O (groups 1 and 5) need a receipt date before the ship date and do
+    // not occur in TPC-H data: their planes run only when a lane of the warp has such a row.
     __device__ __forceinline__ void add_quad(const Quad& x) {
         if constexpr (!kWideQty) {
+            if constexpr (G == 6) {
+                gq[0].add_quad(x.OH, 0u, x);
+                gq[2].add_quad(x.OH, 2u, x);
+                gq[3].add_quad(x.OH, 3u, x);
+                gq[4].add_quad(x.OH, 4u, x);
+                if (__any_sync(0xffffffffu, x.OH & 0x22222222u)) {
+                    gq[1].add_quad(x.OH, 1u, x);
+                    gq[5].add_quad(x.OH, 5u, x);
+                }
+            } else {
 #pragma unroll
-            for (int i = 0; i < G; ++i) gq[i].add_quad(x.OH, (uint32_t)i, x);
+                for (int i = 0; i < G; ++i) gq[i].add_quad(x.OH, (uint32_t)i, x);
+            }
         }
     }
     __device__ __forceinline__ void fold() {
