@@ -36,10 +36,13 @@ namespace gk {
 
 constexpr uint32_t R = ka::R;         // rows per tile
 constexpr uint32_t S = 4;             // ring stages
-constexpr uint32_t W = 8;             // consumer warps
+// consumer warps: 8 for the register planes (128 registers a thread), 16 for the shared-table and
+// global placements, whose atomics need more warps in flight to hide their latency
+template <int P>
+__host__ __device__ constexpr uint32_t consumer_warps() { return P == kPlaceInRegistersPerThread ? 8u : 16u; }
 constexpr uint32_t kStage = ka::kStageBytes;
 constexpr uint32_t kSteps = R / 4;    // 4 rows per consumer step
-static_assert(kSteps % (W * 32) == 0, "steps must divide evenly");
+static_assert(kSteps % (16 * 32) == 0, "steps must divide evenly");
 static_assert(kStage % 16 == 0, "stage alignment");
 
 // Table engine of the shared_mem_per_thread placement.
@@ -74,8 +77,10 @@ struct GroupKeyParams {
 
 // P: placement; NG: plane groups of in_registers_per_thread (4 or 8).
 template <int P, int NG>
-__global__ void __launch_bounds__((gk::W + 1) * 32, 1) q1_groupkey_kernel(const __grid_constant__ GroupKeyParams prm) {
+__global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
+    q1_groupkey_kernel(const __grid_constant__ GroupKeyParams prm) {
     using namespace gk;
+    constexpr uint32_t W = consumer_warps<P>();
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t full_bar[S];
     __shared__ __align__(8) uint64_t empty_bar[S];
@@ -242,7 +247,7 @@ static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_bl
     uint64_t cap = (uint64_t)sm_count;
     if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
     if (blocks > cap) blocks = cap;
-    q1_groupkey_kernel<P, NG><<<(unsigned)blocks, (W + 1) * 32, dyn, st>>>(prm);
+    q1_groupkey_kernel<P, NG><<<(unsigned)blocks, (consumer_warps<P>() + 1) * 32, dyn, st>>>(prm);
     return cudaGetLastError();
 }
 
