@@ -39,7 +39,10 @@ namespace bk {
 
 constexpr uint32_t R = ka::R;   // 2048 rows per tile
 constexpr uint32_t S = 4;
-constexpr uint32_t W = 8;
+// consumer warps: 8 in the register-planes kernel (128 registers a thread), 16 in the table
+// kernel, whose shared-memory atomics need more warps in flight
+template <bool kRegs>
+__host__ __device__ constexpr uint32_t consumer_warps() { return kRegs ? 8u : 16u; }
 constexpr uint32_t kStage = ka::kStageBytes;
 constexpr uint32_t kSteps = R / 4;
 constexpr uint32_t kKindFull = 0, kKindPartial = 1, kKindEnd = 2;
@@ -74,7 +77,7 @@ struct Current {
 // flushing the engine's accumulators whenever the instance changes and at the end. `k` is the
 // running stage counter shared by all engines of the CTA; returns false if a bounded wait
 // expired (the kernel then stops).
-template <int E>
+template <int E, uint32_t W>
 __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t ring, uint8_t* tab, uint64_t* full_bar,
                                                uint64_t* empty_bar, const StageMeta* meta, uint32_t& k,
                                                ka::ConsumerBarrier& cb, uint32_t& bad) {
@@ -176,27 +179,36 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
     return ok;
 }
 
-// Engine a CTA starts with: the role ranges of the grid, then every other engine in turn.
-__device__ __forceinline__ uint32_t first_engine(const BatchParams& prm) {
-    uint32_t e = 0;
-    while (e + 1 < kEngines && blockIdx.x >= prm.role_end[e]) ++e;
-    return e;
+// Engine queue processed at step `step` of a CTA, and the engine code that processes it. The
+// register-planes kernel has one step (queue 0). The table kernel starts at its role's queue
+// among 1..4 (grid ranges role_end), visits the others in turn, then helps with queue 0 through
+// the (group, discount, tax) cells, which hold any instance of <= 4 groups.
+template <bool kRegs>
+__device__ __forceinline__ uint32_t queue_at(const BatchParams& prm, uint32_t step) {
+    if (kRegs) return kEngRegisters;
+    uint32_t e0 = 1;
+    while (e0 + 1 < kEngines && blockIdx.x >= prm.role_end[e0]) ++e0;
+    return step < kEngines - 1 ? 1u + (e0 - 1u + step) % (kEngines - 1u) : (uint32_t)kEngRegisters;
 }
+template <bool kRegs>
+__host__ __device__ constexpr uint32_t steps() { return kRegs ? 1u : kEngines; }
 
 }  // namespace bk
 
-__global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __grid_constant__ BatchParams prm) {
+template <bool kRegs>
+__global__ void __launch_bounds__((bk::consumer_warps<kRegs>() + 1) * 32, 1)
+    q1_batch_kernel(const __grid_constant__ BatchParams prm) {
     using namespace bk;
+    constexpr uint32_t W = consumer_warps<kRegs>();
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t full_bar[S];
     __shared__ __align__(8) uint64_t empty_bar[S];
     __shared__ StageMeta meta[S];
-    __shared__ __align__(8) uint64_t consumers_bar;   // barrier of the 8 consumer warps (bounded wait)
+    __shared__ __align__(8) uint64_t consumers_bar;   // barrier of the consumer warps (bounded wait)
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t ring = smem_addr(smem);
-    uint8_t* const tab = smem + S * kStage;   // shared table, all zero between instances
-    const uint32_t e0 = first_engine(prm);
+    uint8_t* const tab = smem + S * kStage;   // shared table (table kernel), all zero between instances
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < S; ++s) {
@@ -206,19 +218,20 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
         mbar_init(smem_addr(&consumers_bar), W);
         fence_mbar_init();
     }
-    for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(tab)[i] = 0;
+    if (!kRegs)
+        for (uint32_t i = threadIdx.x; i < kTableBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(tab)[i] = 0;
     __syncthreads();
 
     if (warp == W) {
         // ------------------------------ producer ----------------------------------------
-        // Engines in the CTA's order; per engine, claim items from its queue until it is empty,
-        // stream their tiles, then post an end-of-engine marker.
+        // Per step, claim items from that queue until it is empty, stream their tiles, then post
+        // an end-of-queue marker.
         if (lane == 0) {
             const uint64_t pol = policy_evict_first();
             uint32_t k = 0;
             bool ok = true;
-            for (uint32_t step = 0; step < kEngines && ok; ++step) {
-                const uint32_t e = (e0 + step) % kEngines;
+            for (uint32_t step = 0; step < steps<kRegs>() && ok; ++step) {
+                const uint32_t e = queue_at<kRegs>(prm, step);
                 const uint32_t count = prm.item_begin[e + 1] - prm.item_begin[e];
                 for (;;) {
                     const uint32_t idx = count ? atomicAdd(prm.cursor + e, 1u) : count;
@@ -253,7 +266,6 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
                     if (!ok) break;
                 }
                 if (!ok) break;
-                // end-of-engine marker
                 const uint32_t s = k % S;
                 if (!mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) {
                     ok = false;
@@ -267,18 +279,23 @@ __global__ void __launch_bounds__((bk::W + 1) * 32, 1) q1_batch_kernel(const __g
         }
     } else {
         // ------------------------------ consumers ---------------------------------------
-        // The same engine order; each engine's loop keeps only its own accumulators live.
+        // The same queue order; each engine's loop keeps only its own accumulators live.
         ka::ConsumerBarrier cb{smem_addr(&consumers_bar), 0};
         uint32_t bad = 0, k = 0;
-        for (uint32_t step = 0; step < kEngines; ++step) {
-            const uint32_t e = (e0 + step) % kEngines;
+        for (uint32_t step = 0; step < steps<kRegs>(); ++step) {
+            const uint32_t e = queue_at<kRegs>(prm, step);
             bool ok;
-            switch (e) {
-                case kEngRegisters: ok = consume_engine<kEngRegisters>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
-                case kEngCube3: ok = consume_engine<kEngCube3>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
-                case kEngCube: ok = consume_engine<kEngCube>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
-                case kEngSlots: ok = consume_engine<kEngSlots>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
-                default: ok = consume_engine<kEngGlobal>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+            if constexpr (kRegs) {
+                ok = consume_engine<kEngRegisters, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad);
+            } else {
+                switch (e) {
+                    case kEngCube: ok = consume_engine<kEngCube, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                    case kEngSlots: ok = consume_engine<kEngSlots, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                    case kEngGlobal: ok = consume_engine<kEngGlobal, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                    default:   // queues 1 and 0
+                        ok = consume_engine<kEngCube3, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad);
+                        break;
+                }
             }
             if (!ok) break;
         }
@@ -340,14 +357,40 @@ cudaError_t launch_batch_zero_outputs(const BatchInstanceDev* inst, const uint64
 }
 
 uint32_t batch_smem_bytes() { return bk::S * bk::kStage + bk::kTableBytes; }
+// The register-planes kernel needs only the ring; asking for more than half the SM's shared
+// memory keeps it at one CTA per SM, like the table kernel.
+static uint32_t batch_regs_smem_bytes() { return 120u * 1024u; }
 
 cudaError_t batch_prepare_launch() {
-    return cudaFuncSetAttribute(q1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem_bytes());
+    cudaError_t e = cudaFuncSetAttribute(q1_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)batch_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(q1_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)batch_regs_smem_bytes());
 }
 
-cudaError_t launch_batch(const BatchParams& prm, uint32_t grid, cudaStream_t stream) {
-    q1_batch_kernel<<<grid, (bk::W + 1) * 32, batch_smem_bytes(), stream>>>(prm);
-    return cudaGetLastError();
+cudaError_t launch_batch(const BatchParams& prm, uint32_t grid_regs, uint32_t grid_tables, cudaStream_t stream,
+                         cudaStream_t aux, cudaEvent_t fork, cudaEvent_t join) {
+    cudaError_t e = cudaSuccess;
+    const bool both = grid_regs && grid_tables;
+    if (both) {
+        if ((e = cudaEventRecord(fork, stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(aux, fork, 0)) != cudaSuccess) return e;
+    }
+    if (grid_regs) {
+        q1_batch_kernel<true><<<grid_regs, (bk::consumer_warps<true>() + 1) * 32, batch_regs_smem_bytes(),
+                                both ? aux : stream>>>(prm);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (grid_tables) {
+        q1_batch_kernel<false><<<grid_tables, (bk::consumer_warps<false>() + 1) * 32, batch_smem_bytes(), stream>>>(prm);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (both) {
+        if ((e = cudaEventRecord(join, aux)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(stream, join, 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_batch_finalize(const BatchInstanceDev* inst, const uint64_t* group_base, uint32_t ninst,

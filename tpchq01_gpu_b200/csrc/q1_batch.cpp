@@ -105,9 +105,9 @@ uint32_t q1::batch_engine(uint32_t mode, uint32_t num_groups) {
 
 namespace {
 
-// Relative cost of a row per engine (time per row of the group-key kernel on a B200, registers =
-// 1): used only to size each engine's share of the grid.
-constexpr double kEngineCost[kEngines] = {1.0, 2.0, 2.3, 3.1, 10.0};
+// Relative cost of a row per engine (time per row of the group-key kernel on a B200, register
+// planes = 1): used only to split the grid.
+constexpr double kEngineCost[kEngines] = {1.0, 1.5, 1.8, 2.1, 10.0};
 
 void plan_items(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, int only, std::vector<BatchItem>& items,
                 uint32_t begin[kEngines + 1]) {
@@ -135,31 +135,42 @@ void plan_items(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, int on
     begin[kEngines] = (uint32_t)items.size();
 }
 
-// CTAs per engine in proportion to the engine's estimated cost (at least one for an engine with
-// work when the grid allows); returns the grid actually used.
-uint32_t plan_roles(const BatchInstanceDev* inst, const std::vector<BatchItem>& items, const uint32_t begin[kEngines + 1],
-                    uint32_t grid, uint32_t role_end[kEngines]) {
-    grid = std::max<uint32_t>(1, std::min<uint32_t>(grid, (uint32_t)items.size()));
-    double cost[kEngines] = {0, 0, 0, 0, 0}, total = 0;
+// Splits `grid` CTAs: the register-planes kernel gets its cost share (a little under, since the
+// table kernel also drains queue 0 once its own queues are empty), the table kernel the rest,
+// divided among queues 1..4 by cost.
+void plan_roles(const std::vector<BatchItem>& items, const uint32_t begin[kEngines + 1], uint32_t grid,
+                BatchParams& prm) {
+    double cost[kEngines] = {0, 0, 0, 0, 0}, total = 0, tables = 0;
     for (uint32_t e = 0; e < kEngines; ++e) {
         for (uint32_t j = begin[e]; j < begin[e + 1]; ++j) cost[e] += (double)items[j].num_tiles * kEngineCost[e];
         total += cost[e];
+        if (e) tables += cost[e];
     }
-    uint32_t share[kEngines] = {0, 0, 0, 0, 0}, used = 0;
-    for (uint32_t e = 0; e < kEngines; ++e) {
+    uint32_t regs = 0;
+    if (cost[0] > 0) {
+        regs = tables > 0 ? (uint32_t)(0.9 * grid * cost[0] / total) : grid;
+        regs = std::max<uint32_t>(1, std::min<uint32_t>(regs, grid - (tables > 0 ? 1 : 0)));
+        regs = std::min<uint32_t>(regs, begin[1] - begin[0]);
+    }
+    const uint32_t tgrid = tables > 0 ? std::max<uint32_t>(1, std::min<uint32_t>(grid - regs, begin[kEngines] - begin[1]))
+                                      : 0;
+    prm.grid_regs = regs;
+    prm.grid_tables = tgrid;
+    // queue shares of the table kernel
+    uint32_t share[kEngines] = {0, 0, 0, 0, 0}, used = 0, big = 1;
+    for (uint32_t e = 1; e < kEngines; ++e) {
         if (cost[e] <= 0) continue;
-        share[e] = std::max<uint32_t>(1, (uint32_t)(grid * cost[e] / (total > 0 ? total : 1)));
+        share[e] = std::max<uint32_t>(1, (uint32_t)(tgrid * cost[e] / (tables > 0 ? tables : 1)));
         used += share[e];
-    }
-    // trim or pad the largest share so the shares sum to the grid
-    uint32_t big = 0;
-    for (uint32_t e = 1; e < kEngines; ++e)
         if (share[e] > share[big]) big = e;
-    if (used > grid) share[big] -= std::min(share[big] - 1, used - grid);
-    else share[big] += grid - used;
+    }
+    if (tgrid) {
+        if (used > tgrid) share[big] -= std::min(share[big] - 1, used - tgrid);
+        else share[big] += tgrid - used;
+    }
+    prm.role_end[0] = 0;
     uint32_t acc = 0;
-    for (uint32_t e = 0; e < kEngines; ++e) role_end[e] = (acc += share[e]);
-    return grid;
+    for (uint32_t e = 1; e < kEngines; ++e) prm.role_end[e] = (acc += share[e]);
 }
 
 }  // namespace
@@ -167,7 +178,7 @@ uint32_t plan_roles(const BatchInstanceDev* inst, const std::vector<BatchItem>& 
 void q1::batch_plan(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, uint32_t grid, std::vector<BatchItem>& items,
                     BatchParams& prm) {
     plan_items(inst, n, std::max<uint32_t>(1, chunk), -1, items, prm.item_begin);
-    plan_roles(inst, items, prm.item_begin, grid, prm.role_end);
+    plan_roles(items, prm.item_begin, grid, prm);
 }
 
 struct q1_batch {
@@ -189,6 +200,15 @@ struct q1_batch {
     bool zero_outputs = true;
     std::string cache;
     DevMem d_inst, d_items, d_base, d_scratch, d_cursor;
+    cudaStream_t aux = nullptr;              // the register-planes kernel runs beside the table kernel
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~q1_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (aux) cudaStreamDestroy(aux);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+    }
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t tuned_classes = 0;
@@ -198,7 +218,8 @@ struct q1_batch {
 static void build_items(q1_batch* b, uint32_t chunk, int only = -1) {
     for (uint32_t i = 0; i < b->n; ++i) b->inst[i].mode = b->modes[i];
     plan_items(b->inst.data(), b->n, std::max<uint32_t>(1, chunk), only, b->items, b->roles.item_begin);
-    b->launch_grid = plan_roles(b->inst.data(), b->items, b->roles.item_begin, b->grid, b->roles.role_end);
+    plan_roles(b->items, b->roles.item_begin, b->grid, b->roles);
+    b->launch_grid = b->roles.grid_regs + b->roles.grid_tables;
 }
 
 static q1_status upload(q1_batch* b) {
@@ -233,7 +254,7 @@ static q1_status enqueue(q1_batch* b, cudaStream_t s) {
         prm.items = static_cast<const BatchItem*>(b->d_items.p);
         prm.cursor = static_cast<uint32_t*>(b->d_cursor.p);
         prm.status = b->di->status;
-        Q1_CUDA(launch_batch(prm, b->launch_grid, s));
+        Q1_CUDA(launch_batch(prm, prm.grid_regs, prm.grid_tables, s, b->aux, b->fork, b->join));
     }
     Q1_CUDA(launch_batch_finalize(static_cast<const BatchInstanceDev*>(b->d_inst.p),
                                   static_cast<const uint64_t*>(b->d_base.p), b->n, b->total_groups, s));
@@ -285,6 +306,11 @@ q1_status q1_batch_create(const q1_batch_instance* in, uint32_t n, const q1_batc
     cudaStream_t s = (cudaStream_t)cuda_stream;
     Q1_CUDA(cudaGetDevice(&b->device));
     q1_status st = device_info(b->device, &b->di);
+    if (st == Q1_OK) {
+        Q1_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+        Q1_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        Q1_CUDA(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
+    }
     if (st != Q1_OK) return st;
     b->n = n;
     b->use_graph = opts ? opts->use_graph != 0 : true;
@@ -481,8 +507,6 @@ q1_status q1_batch_instance_mode(q1_batch* b, uint32_t i, int32_t* mode) {
 
 q1_status q1_batch_destroy(q1_batch* b) {
     if (!b) return Q1_OK;
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
     delete b;
     return Q1_OK;
 }

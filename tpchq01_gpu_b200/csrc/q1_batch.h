@@ -47,24 +47,31 @@ enum BatchEngine : uint32_t {
 };
 uint32_t batch_engine(uint32_t mode, uint32_t num_groups);
 
+// One execution runs two persistent kernels side by side: the register-planes kernel (queue 0)
+// and the table kernel (queues 1..4, then it helps with queue 0 through the cells engine).
 struct BatchParams {
     const BatchInstanceDev* inst;
     const BatchItem* items;             // grouped by engine: [item_begin[e], item_begin[e + 1])
     uint32_t item_begin[kEngines + 1];
-    uint32_t role_end[kEngines];        // CTAs [role_end[e-1], role_end[e]) start with engine e
+    uint32_t role_end[kEngines];        // table kernel: CTAs [role_end[e-1], role_end[e]) start
+                                        // with queue e (e = 1..4; role_end[0] = 0)
+    uint32_t grid_regs, grid_tables;    // CTAs of the two kernels (a zero grid skips a kernel)
     uint32_t* cursor;                   // kEngines claim counters, zeroed before every launch
     uint32_t* status;
 };
 
 // Cuts every instance (host descriptors) into items of at most `chunk` tiles, groups them by
-// engine (largest first inside an engine) and gives each engine a share of the `grid` CTAs in
-// proportion to its estimated cost; fills prm.item_begin and prm.role_end.
+// engine (largest first inside an engine), splits the `grid` CTAs between the two kernels and
+// the table kernel's among queues 1..4, in proportion to estimated cost.
 void batch_plan(const BatchInstanceDev* inst, uint32_t n, uint32_t chunk, uint32_t grid, std::vector<BatchItem>& items,
                 BatchParams& prm);
 
 uint32_t batch_smem_bytes();
 cudaError_t batch_prepare_launch();
-cudaError_t launch_batch(const BatchParams& prm, uint32_t grid, cudaStream_t stream);
+// Launches the kernels of prm.grid_regs / prm.grid_tables; when both run, the register-planes
+// kernel goes to `aux`, forked from and joined back into `stream` with the two events.
+cudaError_t launch_batch(const BatchParams& prm, uint32_t grid_regs, uint32_t grid_tables, cudaStream_t stream,
+                         cudaStream_t aux, cudaEvent_t fork, cudaEvent_t join);
 cudaError_t launch_batch_zero_outputs(const BatchInstanceDev* inst, const uint64_t* group_base, uint32_t ninst,
                                       uint64_t total_groups, cudaStream_t stream);
 cudaError_t launch_batch_finalize(const BatchInstanceDev* inst, const uint64_t* group_base, uint32_t ninst,

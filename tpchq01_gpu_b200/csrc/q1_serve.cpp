@@ -233,6 +233,8 @@ struct q1_server {
     DeviceInfo* di = nullptr;
     cudaStream_t stream = nullptr;         // rounds
     cudaStream_t plain_stream = nullptr;   // q1_server_plain
+    cudaStream_t aux = nullptr;            // the batch's register-planes kernel
+    cudaEvent_t fork = nullptr, join = nullptr;
     q1_server_opts opts{};
 
     // resident table: ship | qty | disc | tax | price | codes | keys
@@ -487,8 +489,7 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
             prm.items = s->d_items.as<BatchItem>();
             prm.cursor = s->d_cursor.as<uint32_t>();
             prm.status = s->di->status;
-            const uint32_t grid = prm.role_end[kEngines - 1];
-            Q1_CUDA(launch_batch(prm, grid, st));
+            Q1_CUDA(launch_batch(prm, prm.grid_regs, prm.grid_tables, st, s->aux, s->fork, s->join));
         }
         Q1_CUDA(launch_batch_finalize(s->d_inst.as<BatchInstanceDev>(), s->d_base.as<uint64_t>(), ninst, groups, st));
     }
@@ -648,6 +649,9 @@ q1_status q1_server_open(const q1_server_opts* opts, q1_server** out) {
     if (st != Q1_OK) return st;
     Q1_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     Q1_CUDA(cudaStreamCreateWithFlags(&s->plain_stream, cudaStreamNonBlocking));
+    Q1_CUDA(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+    Q1_CUDA(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+    Q1_CUDA(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
     Q1_CUDA(batch_prepare_launch());
     s->res_rows = s->opts.resident_rows;
     if ((st = build_resident(s.get())) != Q1_OK) return st;
@@ -860,6 +864,9 @@ q1_status q1_server_close(q1_server* s) {
         cudaStreamSynchronize(s->plain_stream);
         cudaStreamDestroy(s->plain_stream);
     }
+    if (s->aux) cudaStreamDestroy(s->aux);
+    if (s->fork) cudaEventDestroy(s->fork);
+    if (s->join) cudaEventDestroy(s->join);
     delete s;
     return Q1_OK;
 }
