@@ -582,6 +582,28 @@ q1_status q1_server_resident_columns(q1_server* server, q1_compressed_columns* c
 /* Finishes queued requests, stops the dispatcher and frees everything. */
 q1_status q1_server_close(q1_server* server);
 
+/* ------------------------------------------------------------------------------------------ */
+/* Failure detection. No reference counterpart (the reference exits on any error,                */
+/* src/main.cu:260-339). Faults are injected on the host; the device side is exercised by a wait */
+/* that nothing completes, bounded like every wait of the kernels.                              */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef enum q1_fault {
+    Q1_FAULT_NONE         = 0,   /* clears every pending fault */
+    Q1_FAULT_CPU_WORKER   = 1,   /* the next CPU pool jobs raise (Q1_ERR_CPU_WORKER from q1_run) */
+    Q1_FAULT_DEVICE_ALLOC = 2,   /* the next context device allocations fail (Q1_ERR_OUT_OF_MEMORY) */
+    Q1_FAULT_PINNED_ALLOC = 3    /* the next context pinned host allocations fail */
+} q1_fault;
+
+/* Makes the next `count` events of `kind` fail (process-wide; for tests of error paths). */
+q1_status q1_inject_fault(q1_fault kind, uint32_t count);
+
+/* Launches one thread that waits on an mbarrier nothing completes, bounded by limit_us
+ * (1 us .. 2 s): the wait expires, the kernel records the timeout in the device status word and
+ * returns, and q1_sync_check(cuda_stream) then reports Q1_ERR_DEVICE_TIMEOUT with the context
+ * still usable. */
+q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream);
+
 /* One-line description of a CUDA device (name, compute capability, SMs, memory, L2) into buf.
  * Replaces get_device_properties / --device (src/helper.hpp:18-48, src/main.cu:266-268). */
 q1_status q1_device_describe(int32_t device, char* buf, size_t buf_len);

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cstring>
 #include <exception>
+#include <stdexcept>
 
 #include "q1_common.cuh"
 #include "q1_internal.h"
@@ -44,6 +45,11 @@ void CpuPool::start(std::function<void(int)> fn) {
     cv_start_.notify_all();
 }
 
+bool CpuPool::failed() {
+    std::lock_guard<std::mutex> lk(m_);
+    return failed_;
+}
+
 bool CpuPool::wait() {
     std::unique_lock<std::mutex> lk(m_);
     cv_done_.wait(lk, [&] { return running_ == 0; });
@@ -63,6 +69,7 @@ void CpuPool::loop(int id) {
         }
         std::string err;
         try {
+            if (take_fault(kFaultCpuWorker)) throw std::runtime_error("injected CPU worker fault");
             job(id);
         } catch (const std::exception& e) {
             err = e.what();

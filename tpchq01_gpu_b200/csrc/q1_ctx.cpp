@@ -80,6 +80,7 @@ struct PinnedBuf {
     q1_status alloc(uint64_t bytes) {
         reset();
         if (!bytes) return Q1_OK;
+        if (take_fault(kFaultPinnedAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected pinned allocation failure");
         cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocDefault);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -102,6 +103,7 @@ struct DevBuf {
     q1_status alloc(uint64_t bytes) {
         reset();
         if (!bytes) return Q1_OK;
+        if (take_fault(kFaultDeviceAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected device allocation failure");
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -801,8 +803,13 @@ static q1_status run_once(q1_ctx* ctx, const q1_params* prm, Agg128* total, doub
             uint64_t off = k * chunk, n = std::min(chunk, gpu_end - off);
             if (pushdown) {
                 FilterChunk fc;
-                if (!ctx->queue.pop(&fc, 120000)) {
-                    st = set_error(Q1_ERR_CPU_WORKER, "filter producer delivered no chunk within 120 s");
+                bool got = false;
+                for (int waited = 0; waited < 120000 && !(got = ctx->queue.pop(&fc, 50)); waited += 50)
+                    if (ctx->pool->failed()) break;   // a producer died: no chunk will come
+                if (!got) {
+                    st = set_error(Q1_ERR_CPU_WORKER, ctx->pool->failed()
+                                                          ? "CPU worker failed: " + ctx->pool->error()
+                                                          : std::string("filter producer delivered no chunk within 120 s"));
                     break;
                 }
                 off = fc.offset;

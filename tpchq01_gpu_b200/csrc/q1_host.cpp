@@ -2,6 +2,8 @@
 // kernel-level launch entry points and the generators.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -597,6 +599,51 @@ q1_status q1_generate_compressed_device(uint64_t seed, uint64_t first_row, uint6
     }
     cudaError_t e = launch_generate_compressed(seed, first_row, rows, g, (cudaStream_t)cuda_stream);
     if (e != cudaSuccess) return cuda_error(e, "generator kernel launch");
+    return Q1_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Fault injection and the bounded-wait self-test
+// ---------------------------------------------------------------------------------------------
+
+namespace q1 {
+namespace {
+std::atomic<uint32_t> g_faults[kFaultKinds];
+}
+bool take_fault(FaultKind kind) {
+    uint32_t v = g_faults[kind].load(std::memory_order_relaxed);
+    while (v) {
+        if (g_faults[kind].compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return true;
+    }
+    return false;
+}
+void set_faults(int kind, uint32_t count) { g_faults[kind].store(count, std::memory_order_relaxed); }
+}  // namespace q1
+
+extern "C" {
+
+q1_status q1_inject_fault(q1_fault kind, uint32_t count) {
+    if (kind == Q1_FAULT_NONE) {
+        for (int k = 1; k < kFaultKinds; ++k) set_faults(k, 0);
+        return Q1_OK;
+    }
+    if (kind < Q1_FAULT_CPU_WORKER || kind > Q1_FAULT_PINNED_ALLOC)
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "unknown fault kind");
+    set_faults((int)kind, count);
+    return Q1_OK;
+}
+
+q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream) {
+    if (limit_us == 0 || limit_us > 2000000) return set_error(Q1_ERR_INVALID_ARGUMENT, "limit must be 1 us .. 2 s");
+    int dev = 0;
+    Q1_CUDA(cudaGetDevice(&dev));
+    DeviceInfo* di = nullptr;
+    q1_status st = device_info(dev, &di);
+    if (st != Q1_OK) return st;
+    cudaError_t e = launch_wait_selftest((uint64_t)limit_us * 1000ull, di->status, (cudaStream_t)cuda_stream);
+    if (e != cudaSuccess) return cuda_error(e, "self-test launch");
     return Q1_OK;
 }
 

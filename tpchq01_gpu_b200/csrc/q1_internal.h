@@ -56,6 +56,11 @@ uint64_t words32(uint64_t rows);   // 1-bit containers
 // CPU coprocessing share (the reference's CoProc / Morsel<KernelX100>, src/cpu.h:23-38)
 // ------------------------------------------------------------------------------------------
 
+// Host-side fault injection (q1_inject_fault): the next `count` events of a kind fail.
+enum FaultKind : int { kFaultCpuWorker = 1, kFaultDeviceAlloc = 2, kFaultPinnedAlloc = 3, kFaultKinds = 4 };
+bool take_fault(FaultKind kind);   // consumes one pending fault of `kind`, if any
+void set_faults(int kind, uint32_t count);
+
 // A fixed pool of worker threads executing morsel-driven jobs.
 class CpuPool {
 public:
@@ -66,6 +71,8 @@ public:
     void start(std::function<void(int)> fn);
     // Returns false if a worker raised an exception (message in error()).
     bool wait();
+    // True once a worker of the current job has raised an exception.
+    bool failed();
     const std::string& error() const { return error_; }
 
 private:

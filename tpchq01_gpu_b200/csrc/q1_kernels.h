@@ -82,6 +82,9 @@ struct GenCompressedOut {
 };
 cudaError_t launch_generate_compressed(uint64_t seed, uint64_t first_row, uint64_t rows, const GenCompressedOut& out,
                                        cudaStream_t stream);
+// One thread waits on an mbarrier nothing completes, bounded by limit_ns; on expiry it records
+// kStatusWaitTimeout in *status and returns (the bounded-wait self-test).
+cudaError_t launch_wait_selftest(uint64_t limit_ns, uint32_t* status, cudaStream_t stream);
 cudaError_t launch_precompute_filter(const uint16_t* shipdate, uint64_t rows, int32_t cutoff_rel, uint32_t* bitmap,
                                      cudaStream_t stream);
 

@@ -5,6 +5,7 @@
 
 #include "q1_common.cuh"
 #include "q1_kernels.h"
+#include "q1_ptx.cuh"
 
 namespace q1 {
 
@@ -73,6 +74,27 @@ __global__ void __launch_bounds__(256) generate_compressed_kernel(uint64_t key, 
         if (out.returnflag) out.returnflag[w16 + i] = rf_w[i];
     }
     if (out.linestatus) out.linestatus[r0 / 32] = ls_w;
+}
+
+__global__ void wait_selftest_kernel(uint64_t limit_ns, uint32_t* status) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t b = ptx::smem_addr(&bar);
+    ptx::mbar_init(b, 1);
+    ptx::fence_mbar_init();
+    // nobody arrives: the phase never completes
+    const uint64_t t0 = ptx::globaltimer();
+    for (uint32_t i = 1;; ++i) {
+        if (ptx::mbar_try_wait(b, 0)) return;
+        if ((i & 63u) == 0 && ptx::globaltimer() - t0 > limit_ns) {
+            atomicOr(status, ptx::kStatusWaitTimeout);
+            return;
+        }
+    }
+}
+
+cudaError_t launch_wait_selftest(uint64_t limit_ns, uint32_t* status, cudaStream_t stream) {
+    wait_selftest_kernel<<<1, 1, 0, stream>>>(limit_ns, status);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_generate_compressed(uint64_t seed, uint64_t first_row, uint64_t rows, const GenCompressedOut& out,
