@@ -274,6 +274,9 @@ def main():
                          "launch vs one plain launch each; serve: Poisson request stream, served vs plain")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--groups", default="4,64,1024,65536", help="groupkey: group counts to sweep")
+    ap.add_argument("--pass-fracs", default="0.01,0.10,0.50,0.98,1.0", help="groupkey: pass fractions to sweep")
+    ap.add_argument("--key-dists", default="uniform,zipf", help="groupkey: key distributions to sweep")
+    ap.add_argument("--placements", default="", help="groupkey: placements to time (default: every one that applies)")
     ap.add_argument("--batch-groups", default="4,64,1024", help="batch: group counts instances draw from")
     ap.add_argument("--tune", type=int, default=1, help="batch: 0 heuristic placements, 1 autotuner")
     ap.add_argument("--ref-gpu", action="store_true",
@@ -591,14 +594,14 @@ def bench_groupkey(args):
     ctx = q.Q1Context()
     ctx.generate(SEED, ROWS, layout="compressed", packing="pair")
     comp, _, rows, _, _ = ctx.table_columns()
-    fracs = [0.01, 0.10, 0.50, 0.98, 1.0]
+    fracs = [float(f) for f in args.pass_fracs.split(",")]
     cutoffs = pass_cutoffs(fracs, SEED)
     keys = torch.empty(rows + 16, dtype=torch.int32, device="cuda")
     points = []
     peak, _ = measured_peaks()
     groups_list = [int(g) for g in args.groups.split(",")]
     for G in groups_list:
-        for dist in ["uniform", "zipf"]:
+        for dist in args.key_dists.split(","):
             cdf = None
             if dist == "zipf":
                 h = np.zeros(G, dtype=np.uint32)
@@ -611,6 +614,8 @@ def bench_groupkey(args):
             out = torch.zeros(G * 12, dtype=torch.int64, device="cuda")
             placements = ([("in_registers_per_thread", 1)] if G <= 8 else []) + [("shared_mem_per_thread", 3),
                                                                                  ("global", 4)]
+            if args.placements:
+                placements = [p_ for p_ in placements if p_[0] in args.placements.split(",")]
             for frac, cutoff in zip(fracs, cutoffs):
                 ref = None
                 for pname, pid in placements:
