@@ -342,12 +342,15 @@ q1_status q1_sync_check(void* cuda_stream);
 /* reference's 6-entry group table (src/constants.hpp:56) to many groups.                      */
 /* ------------------------------------------------------------------------------------------ */
 
-/* Bytes of device scratch q1_launch_groupkey needs for num_groups groups. */
+/* Bytes of device scratch q1_launch_groupkey needs for num_groups groups: 64 per group, plus
+ * about 1.1 GB of partition workspace above 2048 groups (independent of the row count). */
 uint64_t q1_groupkey_scratch_bytes(uint32_t num_groups);
 
 /* Placements: IN_REGISTERS_PER_THREAD (num_groups <= 8; per-thread byte-plane sums),
- * SHARED_MEM_PER_THREAD (a per-CTA shared-memory table: (group, discount) cells for
- * num_groups <= 256, else one slot per key < 2048 with larger keys spilled to global atomics),
+ * SHARED_MEM_PER_THREAD (per-CTA shared-memory tables: (group, discount, tax) cells for
+ * num_groups <= 64, (group, discount) cells for <= 256, one slot per group for <= 2048; above
+ * that the passing rows are first partitioned by key into 8-byte records, 2^27 rows at a time,
+ * and each partition of 4096 keys is then aggregated in a shared-memory slot table),
  * GLOBAL (global atomics for every row). Reads ship, qty, disc, tax, price of dev_cols and dev_keys; the result
  * accumulates into dev_aggregates[num_groups][6] (caller-zeroed int128). dev_scratch: device
  * memory of q1_groupkey_scratch_bytes(num_groups), owned by the caller; calls on different

@@ -12,8 +12,12 @@
 //   in_registers_per_thread  num_groups <= 8: per-thread dp4a byte planes (PlaneRegs<4|8>)
 //   shared_mem_per_thread    num_groups <= 64: shared (group, discount, tax) cells
 //                            (Cube3Table); <= 256: shared (group, discount) cells (CubeTable);
-//                            otherwise keys < 2048 in shared slots (SlotTable), larger keys
-//                            reduced straight into the global accumulators
+//                            <= 4096: shared per-group slots (SlotTable, 3-stage ring above
+//                            2048 groups); above that either this kernel with keys < 4096 in
+//                            slots and larger keys reduced straight into the global
+//                            accumulators, or the two-pass partitioned path of
+//                            groupkey_part.cu, chosen on the device from a sample of the rows
+//                            (q1_groupkey_choose)
 //   global                   every passing row reduces into the global accumulators
 //
 // Accumulators live in scratch memory (per launch, zeroed first): per group 8 x u64 (see
@@ -22,6 +26,9 @@
 // buffer). Launches are capped at 2^31 rows so every u64 scratch sum stays exact.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <cstdlib>
+#include <cstring>
 
 #include "q1_common.cuh"
 #include "q1_keyagg.cuh"
@@ -35,7 +42,9 @@ using namespace ptx;
 namespace gk {
 
 constexpr uint32_t R = ka::R;         // rows per tile
-constexpr uint32_t S = 4;             // ring stages
+constexpr uint32_t kMaxStages = 4;    // ring stages (3 when the table needs the room)
+constexpr uint32_t kWideSlots = 4096; // slot-table keys of the single-pass kernel
+constexpr uint32_t kMaxDynSmem = 227 * 1024;
 // consumer warps: 8 for the register planes (128 registers a thread), 16 for the shared-table and
 // global placements, whose atomics need more warps in flight to hide their latency
 template <int P>
@@ -57,10 +66,13 @@ __host__ __device__ constexpr uint32_t table_kind(int placement, uint32_t num_gr
 __host__ __device__ constexpr uint32_t table_bytes(uint32_t kind, uint32_t num_groups) {
     return kind == kTableCube3 ? ka::cube3_bytes(num_groups)
                                : (kind == kTableCube ? ka::cube_bytes(num_groups)
-                                                     : (kind == kTableSlots ? ka::slot_bytes(num_groups < ka::kSlots
+                                                     : (kind == kTableSlots ? ka::slot_bytes(num_groups < kWideSlots
                                                                                                  ? num_groups
-                                                                                                 : ka::kSlots)
+                                                                                                 : kWideSlots)
                                                                             : 0u));
+}
+__host__ __device__ constexpr uint32_t ring_stages(uint32_t kind, uint32_t num_groups) {
+    return kMaxStages * ka::kStageBytes + table_bytes(kind, num_groups) <= kMaxDynSmem ? kMaxStages : kMaxStages - 1;
 }
 
 }  // namespace gk
@@ -71,8 +83,11 @@ struct GroupKeyParams {
     int32_t cutoff;                 // cutoff_day - 727563
     uint32_t num_groups;
     uint32_t table;                 // gk::TableKind
+    uint32_t stages;                // ring stages
     unsigned long long* acc;        // scratch: num_groups x 8 u64, zeroed
     uint32_t* status;
+    const uint32_t* mode;           // when set, the kernel runs only if *mode == mode_want
+    uint32_t mode_want;
 };
 
 // P: placement; NG: plane groups of in_registers_per_thread (4 or 8).
@@ -82,9 +97,11 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
     using namespace gk;
     constexpr uint32_t W = consumer_warps<P>();
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t full_bar[S];
-    __shared__ __align__(8) uint64_t empty_bar[S];
+    __shared__ __align__(8) uint64_t full_bar[kMaxStages];
+    __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
     __shared__ __align__(8) uint64_t cons_bar;
+    if (prm.mode && *prm.mode != prm.mode_want) return;   // the other path of a chosen pair runs
+    const uint32_t S = prm.stages;
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint64_t num_tiles = prm.rows / R;
@@ -93,7 +110,7 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
     ka::Cube3Table cube3;
     ka::CubeTable cube;
     ka::SlotTable slots;
-    const uint32_t hot = G < ka::kSlots ? G : ka::kSlots;
+    const uint32_t hot = G < kWideSlots ? G : kWideSlots;
     if (P == kPlaceSharedMemPerThread) {
         if (prm.table == kTableCube3) cube3.bind(smem + S * kStage, G);
         else if (prm.table == kTableCube) cube.bind(smem + S * kStage, G);
@@ -238,7 +255,7 @@ __global__ void __launch_bounds__(256) q1_groupkey_finalize(const unsigned long 
 template <int P, int NG>
 static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_blocks, cudaStream_t st) {
     using namespace gk;
-    const uint32_t dyn = S * kStage + table_bytes(prm.table, prm.num_groups);
+    const uint32_t dyn = prm.stages * kStage + table_bytes(prm.table, prm.num_groups);
     cudaError_t e =
         cudaFuncSetAttribute(q1_groupkey_kernel<P, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
@@ -251,11 +268,65 @@ static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_bl
     return cudaGetLastError();
 }
 
+static uint64_t acc_bytes(uint32_t num_groups) { return 64ull * num_groups; }
+static bool two_paths(int placement, uint32_t num_groups) {
+    return placement == kPlaceSharedMemPerThread && num_groups >= groupkey_part_min_groups();
+}
+
+// For more than 4096 groups in the shared placement, picks one of two exact paths from 8192
+// evenly spaced sample rows and writes it to *mode:
+//   kModeSinglePass   the group-key kernel: keys < 4096 in a shared slot table, passing rows of
+//                     larger ("cold") keys straight into the global accumulators;
+//   kModePartitioned  the two-pass radix partition (groupkey_part.cu).
+// Cost model fitted to both paths on a B200 (ms per 600 M rows; c = fraction of the rows that
+// pass with a cold key, p = fraction that pass): single pass 2.2 + 20 c + 0.3 p; partitioned
+// 1.7 + 4.3 c + 5.65 (p - c), the hot rows costing more there because skewed keys contend for
+// the same ring counters and slots. The single pass wins when 21.35 c - 5.35 p < -0.5: skewed
+// keys with many passing rows. Both paths give identical results.
+__global__ void __launch_bounds__(256) q1_groupkey_choose(const uint16_t* __restrict__ ship,
+                                                          const uint32_t* __restrict__ keys, uint64_t rows,
+                                                          int32_t cutoff, uint32_t hot, uint32_t force,
+                                                          uint32_t* mode) {
+    constexpr uint32_t K = 8192;
+    if (force) {
+        if (threadIdx.x == 0) *mode = force;
+        return;
+    }
+    __shared__ uint32_t cnt[2];
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t pass = 0, cold = 0;
+    for (uint32_t j = threadIdx.x; j < K; j += blockDim.x) {
+        const uint64_t i = (uint64_t)j * rows / K;
+        if ((int32_t)ship[i] <= cutoff) {
+            ++pass;
+            cold += keys[i] >= hot ? 1u : 0u;
+        }
+    }
+    atomicAdd(&cnt[0], pass);
+    atomicAdd(&cnt[1], cold);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int64_t score = 2135ll * cnt[1] - 535ll * cnt[0];   // 100 x (21.35 c - 5.35 p) x K
+        *mode = score < -50ll * K ? kModeSinglePass : kModePartitioned;
+    }
+}
+
 cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_t rows, int32_t cutoff_rel,
                             uint32_t num_groups, unsigned long long* scratch, unsigned long long* out,
                             uint32_t* status, int sm_count, int max_blocks, cudaStream_t stream) {
-    cudaError_t e = cudaMemsetAsync(scratch, 0, groupkey_scratch_bytes(num_groups), stream);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, acc_bytes(num_groups), stream);
     if (e != cudaSuccess) return e;
+    uint8_t* workspace = reinterpret_cast<uint8_t*>(scratch) + ((acc_bytes(num_groups) + 255) & ~255ull);
+    uint32_t* mode = two_paths(placement, num_groups)
+                         ? reinterpret_cast<uint32_t*>(workspace + groupkey_part_mode_offset())
+                         : nullptr;
+    // Q1_GROUPKEY_PATH=single|partitioned overrides the sample-based choice (tests and tuning)
+    uint32_t force = 0;
+    if (const char* env = std::getenv("Q1_GROUPKEY_PATH")) {
+        if (!std::strcmp(env, "single")) force = kModeSinglePass;
+        else if (!std::strcmp(env, "partitioned")) force = kModePartitioned;
+    }
     const uint64_t kMaxRows = 1ull << 31;
     for (uint64_t off = 0; off < rows; off += kMaxRows) {
         GroupKeyParams prm{};
@@ -266,8 +337,17 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
         prm.cutoff = cutoff_rel;
         prm.num_groups = num_groups;
         prm.table = gk::table_kind(placement, num_groups);
+        prm.stages = gk::ring_stages(prm.table, num_groups);
         prm.acc = scratch;
         prm.status = status;
+        if (mode) {
+            q1_groupkey_choose<<<1, 256, 0, stream>>>(reinterpret_cast<const uint16_t*>(prm.col[0]),
+                                                      reinterpret_cast<const uint32_t*>(prm.col[5]), n, cutoff_rel,
+                                                      gk::kWideSlots, force, mode);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            prm.mode = mode;
+            prm.mode_want = kModeSinglePass;
+        }
         switch (placement) {
             case kPlaceInRegistersPerThread:
                 e = num_groups <= 4 ? launch_gk<kPlaceInRegistersPerThread, 4>(prm, sm_count, max_blocks, stream)
@@ -278,20 +358,30 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
             default: return cudaErrorInvalidValue;
         }
         if (e != cudaSuccess) return e;
+        if (mode) {
+            e = launch_groupkey_part(prm.col, n, cutoff_rel, num_groups, scratch, workspace, mode, status, sm_count,
+                                     max_blocks, stream);
+            if (e != cudaSuccess) return e;
+        }
         // fold after every 2^31-row launch so the scratch sums stay exact
         q1_groupkey_finalize<<<(num_groups + 255) / 256, 256, 0, stream>>>(scratch, num_groups, out);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (off + kMaxRows < rows) {
-            e = cudaMemsetAsync(scratch, 0, groupkey_scratch_bytes(num_groups), stream);
+            e = cudaMemsetAsync(scratch, 0, acc_bytes(num_groups), stream);
             if (e != cudaSuccess) return e;
         }
     }
-    if (rows == 0) return cudaSuccess;
     return cudaSuccess;
 }
 
-uint64_t groupkey_scratch_bytes(uint32_t num_groups) { return 64ull * num_groups; }
+// The accumulators; for more than 4096 groups (two paths of the shared placement) also the
+// partition workspace after them.
+uint64_t groupkey_scratch_bytes(uint32_t num_groups) {
+    return num_groups >= groupkey_part_min_groups()
+               ? ((acc_bytes(num_groups) + 255) & ~255ull) + groupkey_part_workspace_bytes()
+               : acc_bytes(num_groups);
+}
 
 // Group keys of the seeded generator: uniform over [0, G) (cdf == nullptr) or by inverse CDF.
 __global__ void __launch_bounds__(256) generate_keys_kernel(uint64_t key, uint64_t first_row, uint64_t rows,

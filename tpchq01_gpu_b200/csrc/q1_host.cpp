@@ -85,6 +85,7 @@ q1_status check_device_status(cudaStream_t stream, uint32_t* status_word) {
     if (bits) {
         Q1_CUDA(cudaMemset(status_word, 0, sizeof(bits)));
         if (bits & 1u) return set_error(Q1_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+        if (bits & 4u) return set_error(Q1_ERR_INTERNAL, "a device work buffer would have overflowed");
         return set_error(Q1_ERR_DOMAIN, "a row is outside the kernel domain (discount > 100, tax > 255, "
                                         "or a value >= 2^32 / negative)");
     }

@@ -66,6 +66,20 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
                             uint32_t num_groups, unsigned long long* scratch, unsigned long long* out,
                             uint32_t* status, int sm_count, int max_blocks, cudaStream_t stream);
 uint64_t groupkey_scratch_bytes(uint32_t num_groups);
+// High-cardinality path of the shared_mem_per_thread placement (groupkey_part.cu): a radix
+// partition by key, then per-partition shared-memory slot tables. acc: num_groups x 8 u64
+// (zeroed by the caller); workspace: groupkey_part_workspace_bytes(), 256-byte aligned. When
+// `mode` is set, every kernel of the path returns at once unless *mode == kModePartitioned.
+enum GroupKeyMode : uint32_t { kModeSinglePass = 1, kModePartitioned = 2 };
+cudaError_t launch_groupkey_part(const uint8_t* const cols[6], uint64_t rows, int32_t cutoff_rel,
+                                 uint32_t num_groups, unsigned long long* acc, uint8_t* workspace,
+                                 const uint32_t* mode, uint32_t* status, int sm_count, int max_blocks,
+                                 cudaStream_t stream);
+uint64_t groupkey_part_workspace_bytes();
+// byte offset of a spare word in the workspace (the mode word of launch_groupkey)
+uint64_t groupkey_part_mode_offset();
+// fewest groups for which the shared placement has the partitioned path
+uint32_t groupkey_part_min_groups();
 cudaError_t launch_generate_keys(uint64_t seed, uint64_t first_row, uint64_t rows, uint32_t num_groups,
                                  const uint32_t* dev_cdf, uint32_t* dev_keys, cudaStream_t stream);
 

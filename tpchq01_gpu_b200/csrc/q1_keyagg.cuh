@@ -14,8 +14,9 @@
 //                  the discounted sums follow exactly at the flush, because the discount of a
 //                  cell is known there: sum (100-d) p = sum_d (100-d) P_d and
 //                  sum (100-d)(100+t) p = sum_d (100-d) (100 P_d + TP_d).
-//   SlotTable      keys < 2048: a shared-memory table per group (count and discount packed,
-//                  quantity, price, disc_price, charge).
+//   SlotTable      one shared-memory slot per key below the table's size (2048 in the batch
+//                  kernel, 4096 in the group-key kernel and the partitioned path): count and
+//                  discount packed, quantity, price, disc_price, charge.
 //   global         every row reduces straight into the scratch accumulators.
 // The shared tables use only 32-bit shared atomics (64-bit shared atomics are far slower);
 // 64-bit sums are kept as (low word, carry word) pairs: the low word's atomic returns the old
@@ -233,6 +234,7 @@ struct CubeTable {
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
         uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4], carry = 0;
+        if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             c[r] = key[r] * kCubeDisc + d[r];
@@ -307,6 +309,7 @@ struct Cube3Table {
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
         uint32_t c[4], vx[4], ox[4], op[4], carry = 0;
+        if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             c[r] = (key[r] * kCubeDisc + d[r]) * kCubeTax + t[r];
@@ -384,6 +387,7 @@ struct SlotTable {
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
         const uint32_t S = slots;
         uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4], carry = 0;
+        if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const uint32_t a = 100u - d[r];
@@ -442,7 +446,8 @@ struct SlotTable {
 // One quad into a shared table (CubeTable or SlotTable): rows in the table's fast domain go to the
 // table, other passing rows with key < num_groups straight to the scratch, passing rows with
 // key >= num_groups make `bad` nonzero.
-// All lanes of the warp call it (the slow path and the carries use warp votes).
+// All lanes of the warp call it (the slow path, the tables' early exit when no lane of the warp
+// has a row to add, and the carries use warp votes).
 template <class Table>
 __device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_t num_groups, uint32_t hot,
                                            unsigned long long* acc, uint32_t& bad) {

@@ -14,6 +14,7 @@ constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 // Status bits written by kernels (OR-ed into a device word the host reads back).
 constexpr uint32_t kStatusWaitTimeout = 1u;
 constexpr uint32_t kStatusDomain = 2u;
+constexpr uint32_t kStatusInternal = 4u;   // a device work buffer would have overflowed
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
