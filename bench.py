@@ -269,7 +269,7 @@ def main():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="scan", choices=["scan", "c1sweep", "groupkey", "batch", "serve"],
+    ap.add_argument("--mode", default="scan", choices=["scan", "c1sweep", "groupkey", "batch", "serve", "tbl"],
                     help="scan: the 600M-row aggregation (default); batch: 256 instances in one persistent "
                          "launch vs one plain launch each; serve: Poisson request stream, served vs plain")
     ap.add_argument("--instances", type=int, default=256)
@@ -295,6 +295,8 @@ def main():
         return bench_batch(args)
     if args.mode == "serve" and args.impl == "ours":
         return bench_serve(args)
+    if args.mode == "tbl" and args.impl == "ours":
+        return bench_tbl(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -461,6 +463,95 @@ def e2e_pinned(q, args):
 # off / on, uncompressed) under every placement, then the host-streamed mode (pinned table) with
 # CPU fractions 0, 0.1, 0.25, 0.5, pushdown off / on. Every result is checked against the first.
 # ------------------------------------------------------------------------------------------
+
+# ------------------------------------------------------------------------------------------
+# --mode tbl: lineitem text ingestion (the reference's lineitem::FromFile path, run when no
+# column cache exists). An SF-1-sized table (6,001,215 rows) written as .tbl text by
+# q1_tbl_format; timed: the GPU parse of device-resident text (q1_tbl_parse_device, text bytes
+# and 38 B/row of columns per pass against HBM), the file path through q1_tbl_read_file (host
+# read, H2D, parse, D2H), and the reference's value types over a 1 M-row sample on one thread.
+# ------------------------------------------------------------------------------------------
+
+def bench_tbl(args):
+    import ctypes
+    import tempfile
+    import numpy as np
+    import torch
+    import tpchq01_gpu_b200 as q
+    from tpchq01_gpu_b200 import _lib
+
+    L = q.lib()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    rows = args.rows if args.rows != ROWS else 6_001_215
+    text = q.tbl_format(q.generate_host(SEED, 0, rows))
+    nbytes = len(text)
+    dev = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda()
+    out = {"shipdate": torch.empty(rows + 1, dtype=torch.int32, device="cuda")}
+    for k in ["returnflag", "linestatus"]:
+        out[k] = torch.empty(rows + 1, dtype=torch.uint8, device="cuda")
+    for k in ["discount", "tax", "extendedprice", "quantity"]:
+        out[k] = torch.empty(rows + 1, dtype=torch.int64, device="cuda")
+    o = _lib.ColumnsOut(*[out[k].data_ptr() for k in ["shipdate", "returnflag", "linestatus", "discount", "tax",
+                                                       "extendedprice", "quantity"]])
+    got = ctypes.c_uint64(0)
+
+    def parse():
+        _lib.check(L.q1_tbl_parse_device(ctypes.c_void_p(dev.data_ptr()), nbytes, ctypes.byref(o), rows,
+                                         ctypes.byref(got), sh))
+
+    for _ in range(max(args.warmup, 3)):
+        parse()
+    steps = max(1, min(args.steps, 20))
+    sampler = ClockSampler(0)
+    sampler.start()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        parse()                      # synchronous: count, scan, parse, read back the row count
+        times.append((time.perf_counter() - t0) * 1e3)
+    clocks = sampler.stop()
+    ms = sorted(times)[len(times) // 2]
+    peak, kind = measured_peaks()
+    moved = nbytes * 2 + rows * 38   # the text is read twice (count, parse), the columns written once
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "lineitem.tbl")
+        with open(path, "wb") as f:
+            f.write(text)
+        q.tbl_read_file(path)        # warm the page cache
+        t0 = time.perf_counter()
+        cols = q.tbl_read_file(path)
+        file_ms = (time.perf_counter() - t0) * 1e3
+    assert len(cols["shipdate"]) == rows
+    ref = None
+    try:
+        sys.path.insert(0, ROOT)
+        from oracle import py_oracle as O
+        if O.ref_available():
+            sample = text[: nbytes * min(rows, 1_000_000) // max(rows, 1)]
+            sample = sample[: sample.rfind(b"\n") + 1]
+            t0 = time.perf_counter()
+            _, srows = O.ref_parse_tbl(sample)
+            ref_s = time.perf_counter() - t0
+            ref = {"rows_per_s": srows / ref_s, "rows": srows, "cores": 1,
+                   "kind": "reference value types (Decimal<15,2>, Char, Date) with the tokenizer restated"}
+    except Exception as e:   # the reference build is optional for this mode
+        ref = {"unavailable": str(e)}
+    line = {"metric": "lineitem .tbl rows parsed per second", "mode": "tbl", "value": rows / (ms / 1e3),
+            "unit": "rows/s", "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"lineitem_tbl_{rows}_rows", "rows": rows, "text_bytes": nbytes,
+                       "bytes_per_row": nbytes / rows},
+            "gpu_parse": {"ms": ms, "text_gbs": nbytes / (ms / 1e3) / 1e9, "moved_gbs": moved / (ms / 1e3) / 1e9,
+                          "frac_hbm": moved / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
+                          "note": "host wall time of the synchronous call (three kernels and two 8-byte reads)"},
+            "file": {"ms": file_ms, "rows_per_s": rows / (file_ms / 1e3),
+                     "note": "q1_tbl_read_file from the page cache: read, H2D, parse, D2H of the columns"},
+            "reference_cpu": ref, "clocks": clocks, "gpu_launches": 3}
+    print(json.dumps(line), flush=True)
+    return 0
+
 
 def bench_c1sweep(args):
     import ctypes

@@ -454,6 +454,39 @@ q1_status q1_cache_load(q1_ctx* ctx, const char* dir, q1_layout layout, q1_flag_
                         q1_residency residency, uint64_t* rows_out);
 
 /* ------------------------------------------------------------------------------------------ */
+/* lineitem text (dbgen .tbl) ingestion on the GPU: replaces lineitem::FromFile                 */
+/* (cpu/tpch_kit.cpp:155-172, TableReader at :10-99), which the reference runs when no column   */
+/* cache exists (src/main.cu:441-475). One row per '\n'-terminated line (the last '\n' may be    */
+/* missing), fields separated by '|'; fields 5-11 are read: quantity, extendedprice, discount,  */
+/* tax as "[+-]int[.frac]" -> 100*int + frac (Decimal<15,2>), returnflag and linestatus as one  */
+/* character, shipdate as "year-month-day" -> MonetDB day number (Date, monetdb.cpp todate).    */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Rows in a device text buffer (16-byte aligned for full speed). Synchronous on cuda_stream. */
+q1_status q1_tbl_count_device(const char* dev_text, uint64_t bytes, uint64_t* rows, void* cuda_stream);
+
+/* Parses a device text buffer into reference-typed device columns of `capacity` rows (row i =
+ * line i). Synchronous; *rows_out = the rows in the text. Q1_ERR_INVALID_ARGUMENT when the text
+ * holds more rows than `capacity` or has malformed lines (their count and the first one's byte
+ * offset in q1_last_error(); those rows are written as zeros). */
+q1_status q1_tbl_parse_device(const char* dev_text, uint64_t bytes, const q1_columns_out* dev_out,
+                              uint64_t capacity, uint64_t* rows_out, void* cuda_stream);
+
+/* Reads a .tbl file through the GPU parser (256 MB chunks of whole lines, on the current
+ * device) into caller-owned host columns of `capacity` rows; out == NULL only counts the rows. */
+q1_status q1_tbl_read_file(const char* path, q1_columns_out* out, uint64_t capacity, uint64_t* rows_out);
+
+/* Loads a .tbl file into the context like q1_load_columns (src/main.cu:441-475). */
+q1_status q1_tbl_load(q1_ctx* ctx, const char* path, q1_layout layout, q1_flag_packing packing,
+                      q1_residency residency, uint64_t* rows_out);
+
+/* Writes host columns as .tbl text (the inverse of the parser, two decimals per value, ISO
+ * dates); the fields Q1 does not read get deterministic placeholders derived from
+ * first_row + i. buf == NULL: only *bytes_out (the text's size) is set. Multi-threaded. */
+q1_status q1_tbl_format(const q1_columns* host_columns, uint64_t first_row, uint64_t rows, char* buf,
+                        uint64_t capacity, uint64_t* bytes_out);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Synthetic data generator (stands in for dbgen, scripts/genlineitem.sh)                       */
 /* ------------------------------------------------------------------------------------------ */
 

@@ -187,3 +187,39 @@ class RefTable:
             self.close()
         except Exception:
             pass
+
+
+def _tbl_cols(rows):
+    return {"shipdate": np.zeros(rows, np.int32), "quantity": np.zeros(rows, np.int64),
+            "extendedprice": np.zeros(rows, np.int64), "discount": np.zeros(rows, np.int64),
+            "tax": np.zeros(rows, np.int64), "returnflag": np.zeros(rows, "S1"), "linestatus": np.zeros(rows, "S1")}
+
+
+def _tbl_ptrs(c):
+    return [ptr(c[k]) for k in ["shipdate", "quantity", "extendedprice", "discount", "tax", "returnflag", "linestatus"]]
+
+
+def parse_tbl(text, capacity=None):
+    """The restatement's .tbl parse: (columns, rows, malformed lines, first malformed byte)."""
+    L = lib()
+    L.oracle_parse_tbl.restype = ctypes.c_uint64
+    L.oracle_parse_tbl.argtypes = [ctypes.c_char_p, ctypes.c_uint64] + [ctypes.c_void_p] * 7 + [
+        ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    if capacity is None:
+        capacity = text.count(b"\n") + 1
+    c = _tbl_cols(capacity)
+    bad, first = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    rows = L.oracle_parse_tbl(text, len(text), *_tbl_ptrs(c), capacity, ctypes.byref(bad), ctypes.byref(first))
+    n = min(rows, capacity)
+    return {k: v[:n] for k, v in c.items()}, rows, bad.value, first.value
+
+
+def ref_parse_tbl(text):
+    """The reference's own value types (Decimal<15,2>, Char, Date) over well-formed .tbl text."""
+    r = ref()
+    r.q1ref_parse_tbl.restype = ctypes.c_uint64
+    r.q1ref_parse_tbl.argtypes = [ctypes.c_char_p, ctypes.c_uint64] + [ctypes.c_void_p] * 7 + [ctypes.c_uint64]
+    capacity = text.count(b"\n") + 1
+    c = _tbl_cols(capacity)
+    rows = r.q1ref_parse_tbl(text, len(text), *_tbl_ptrs(c), capacity)
+    return {k: v[:rows] for k, v in c.items()}, rows

@@ -168,3 +168,108 @@ int oracle_compress_separate(const int32_t* shipdate, const int64_t* discount, c
     }
     return bad;
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * lineitem text (.tbl) parsing, restated from lineitem::FromFile (cpu/tpch_kit.cpp:155-172):
+ *   - one row per line, fields split at '|' (TableReader::tokenize, cpu/tpch_kit.cpp:26-57);
+ *     fields 5-11 (1-based) read, the rest skipped;
+ *   - decimals "[+-]int[.frac]" -> 100 * int + frac, the fraction's digits read as an integer
+ *     (BaseDecimal::parse + Decimal<15,2>::ToValue, cpu/tpch_kit.cpp:100-121, tpch_kit.hpp:52-80);
+ *   - characters: exactly one byte (Char, cpu/tpch_kit.hpp:15-23);
+ *   - dates "year-month-day" -> day number counted like MonetDB's todate (cpu/monetdb.cpp):
+ *     365 * y + leap years before y (+1 for the year-0 convention) + days before the month
+ *     (+1 after February of a leap year) + day - 1; 1992-01-01 -> 727563.
+ * A line that does not match is malformed: its row is zeroed and counted in *bad, the byte
+ * offset of the first one in *first_bad. Returns the number of rows (lines; a final '\n' starts
+ * none); rows beyond `capacity` are counted as malformed and not written.
+ * ------------------------------------------------------------------------------------------- */
+static int tbl_int(const char* t, uint64_t n, uint64_t* p, int64_t* v) {
+    int neg = 0;
+    if (*p < n && (t[*p] == '+' || t[*p] == '-')) neg = t[(*p)++] == '-';
+    int64_t x = 0;
+    int nd = 0;
+    while (*p < n && t[*p] >= '0' && t[*p] <= '9') {
+        if (++nd > 18) return 0;
+        x = x * 10 + (t[(*p)++] - '0');
+    }
+    *v = neg ? -x : x;
+    return nd > 0;
+}
+
+static int tbl_dec(const char* t, uint64_t n, uint64_t* p, int64_t* v) {
+    int64_t i = 0, f = 0;
+    if (!tbl_int(t, n, p, &i)) return 0;
+    if (*p < n && t[*p] == '.') {
+        ++*p;
+        if (!tbl_int(t, n, p, &f)) return 0;
+    }
+    *v = 100 * i + f;
+    return 1;
+}
+
+static int tbl_sep(const char* t, uint64_t n, uint64_t* p) {
+    if (*p >= n || t[*p] != '|') return 0;
+    ++*p;
+    return 1;
+}
+
+static int32_t tbl_day(int64_t y, int64_t m, int64_t d) {
+    static const int mdays[13] = {0, 31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+    static const int before[13] = {0, 0, 31, 59, 90, 120, 151, 181, 212, 243, 273, 304, 334};
+    if (y < 1 || y > 999999 || m < 1 || m > 12 || d < 1) return -1;
+    const int leap = (y % 4 == 0) && (y % 100 != 0 || y % 400 == 0);
+    if (d > mdays[m] + ((m == 2 && leap) ? 1 : 0)) return -1;
+    const int64_t q = y - 1;
+    return (int32_t)(365 * y + (q / 4 - q / 100 + q / 400 + 1) + before[m] + ((m > 2 && leap) ? 1 : 0) + d - 1);
+}
+
+static int tbl_line(const char* t, uint64_t n, uint64_t p, int32_t* ship, int64_t* q, int64_t* pr, int64_t* di,
+                    int64_t* tx, char* rf, char* ls) {
+    for (int f = 0; f < 4; ++f) {
+        while (p < n && t[p] != '|' && t[p] != '\n') ++p;
+        if (!tbl_sep(t, n, &p)) return 0;
+    }
+    if (!tbl_dec(t, n, &p, q) || !tbl_sep(t, n, &p) || !tbl_dec(t, n, &p, pr) || !tbl_sep(t, n, &p) ||
+        !tbl_dec(t, n, &p, di) || !tbl_sep(t, n, &p) || !tbl_dec(t, n, &p, tx) || !tbl_sep(t, n, &p))
+        return 0;
+    if (p >= n || t[p] == '|' || t[p] == '\n') return 0;
+    *rf = t[p++];
+    if (!tbl_sep(t, n, &p) || p >= n || t[p] == '|' || t[p] == '\n') return 0;
+    *ls = t[p++];
+    if (!tbl_sep(t, n, &p)) return 0;
+    int64_t y, m, d;
+    if (!tbl_int(t, n, &p, &y) || p >= n || t[p++] != '-' || !tbl_int(t, n, &p, &m) || p >= n || t[p++] != '-' ||
+        !tbl_int(t, n, &p, &d))
+        return 0;
+    if (p < n && t[p] != '|' && t[p] != '\n') return 0;
+    if (m > 31 || d > 31) return 0;
+    *ship = tbl_day(y, m, d);
+    return *ship >= 0;
+}
+
+uint64_t oracle_parse_tbl(const char* text, uint64_t bytes, int32_t* ship, int64_t* qty, int64_t* price,
+                          int64_t* disc, int64_t* tax, char* rf, char* ls, uint64_t capacity, uint64_t* bad,
+                          uint64_t* first_bad) {
+    uint64_t row = 0, start = 0;
+    *bad = 0;
+    *first_bad = ~0ull;
+    while (start < bytes) {
+        uint64_t end = start;
+        while (end < bytes && text[end] != '\n') ++end;
+        int32_t s = 0;
+        int64_t q = 0, pr = 0, di = 0, tx = 0;
+        char a = 0, b = 0;
+        const int ok = tbl_line(text, bytes, start, &s, &q, &pr, &di, &tx, &a, &b);
+        if (row < capacity) {
+            if (!ok) s = 0, q = pr = di = tx = 0, a = b = 0;
+            ship[row] = s, qty[row] = q, price[row] = pr, disc[row] = di, tax[row] = tx, rf[row] = a, ls[row] = b;
+        }
+        if (!ok || row >= capacity) {
+            ++*bad;
+            if (start < *first_bad) *first_bad = start;
+        }
+        ++row;
+        start = end + 1;
+    }
+    return row;
+}

@@ -5,6 +5,7 @@
 //
 // Kernels exposed:
 //   KernelHyPer<true>                    cpu/kernel_hyper.hpp:6-96 (tuple at a time, int128 sums)
+//   lineitem text values                 Decimal<15,2> / Char / Date (cpu/tpch_kit.hpp, .cpp)
 //   KernelX100<kMagic,true,kNoAvx512>    cpu/kernel_x100.hpp:16-405 (vectorised, partial shuffle)
 // The reference's own multi-threaded driver, Morsel<> (cpu/kernel_x100.hpp:423-665), returns
 // from wait() before the last morsel and the per-thread merges have finished (it compares a
@@ -277,6 +278,50 @@ int q1ref_pool_run(void* pool, uint64_t offset, uint64_t num, uint64_t morsel, i
 }
 
 int q1ref_pool_threads(void* pool) { return (int)((X100Pool*)pool)->workers.size(); }
+
+// lineitem text through the reference's own value types: each line is split at '|' the way
+// TableReader::tokenize does (cpu/tpch_kit.cpp:26-57; restated here because tpch_kit.cpp also
+// holds the boost-based parsers), and fields 5-11 are converted by the reference's
+// Decimal<15,2>, Char and Date constructors (cpu/tpch_kit.hpp:15-80, cpu/tpch_kit.cpp:142-153)
+// exactly as lineitem::FromFile pushes them (cpu/tpch_kit.cpp:155-172). Only for well-formed
+// text: the reference asserts on anything else. Returns the rows parsed.
+uint64_t q1ref_parse_tbl(const char* text, uint64_t bytes, int32_t* ship, int64_t* qty, int64_t* price,
+                         int64_t* disc, int64_t* tax, char* rf, char* ls, uint64_t capacity) {
+    std::vector<char> line;
+    uint64_t row = 0, start = 0;
+    while (start < bytes && row < capacity) {
+        uint64_t end = start;
+        while (end < bytes && text[end] != '\n') ++end;
+        line.assign(text + start, text + end);
+        line.push_back('\0');
+        const char* w[11];
+        int64_t len[11];
+        int nw = 0;
+        int64_t ws = 0;
+        for (int64_t i = 0; nw < 11; ++i) {
+            const char c = line[i];
+            if (c == '|' || c == '\0') {
+                w[nw] = &line[ws];
+                len[nw] = i - ws;
+                line[i] = '\0';
+                ws = i + 1;
+                ++nw;
+                if (c == '\0') break;
+            }
+        }
+        if (nw < 11) break;
+        qty[row] = Decimal<15, 2>(w[4], len[4]).dec_val;
+        price[row] = Decimal<15, 2>(w[5], len[5]).dec_val;
+        disc[row] = Decimal<15, 2>(w[6], len[6]).dec_val;
+        tax[row] = Decimal<15, 2>(w[7], len[7]).dec_val;
+        rf[row] = Char(w[8], len[8]).chr_val;
+        ls[row] = Char(w[9], len[9]).chr_val;
+        ship[row] = Date(w[10], len[10]).dte_val;
+        ++row;
+        start = end + 1;
+    }
+    return row;
+}
 
 void q1ref_pool_free(void* pool) {
     X100Pool* p = (X100Pool*)pool;

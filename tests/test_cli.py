@@ -70,3 +70,29 @@ def test_data_dir_layout_of_the_reference(cuda, tmp_path):
              "--runs=1"], tmp_path)
     assert r.returncode == 0, r.stderr
     assert os.path.exists(tmp_path / "data" / "0.010000" / "shipdate.bin")
+
+
+@pytest.mark.gpu
+def test_tbl_path_of_the_reference(cuda, tmp_path):
+    """Without a column cache, D/<sf>/lineitem.tbl is parsed (on the GPU) and the cache written,
+    as the reference does (src/main.cu:441-475); the tables printed from the text, from the cache
+    it left and from --tbl agree with the generator's."""
+    common = ["--apply-compression", "--print-results", "--runs=1", "--sf=0.05", "--seed=7"]
+    data = str(tmp_path / "data")
+    made = run(common + ["--data-dir=" + data, "--write-tbl"], tmp_path)
+    assert made.returncode == 0, made.stderr
+    tbl = tmp_path / "data" / "0.050000" / "lineitem.tbl"
+    assert tbl.exists() and not (tmp_path / "data" / "0.050000" / "shipdate.bin").exists()
+    parsed = run(common + ["--data-dir=" + data], tmp_path)
+    assert parsed.returncode == 0, parsed.stderr
+    assert "Parsing the lineitem table" in parsed.stdout
+    assert (tmp_path / "data" / "0.050000" / "shipdate.bin").exists()
+    cached = run(common + ["--data-dir=" + data], tmp_path)
+    direct = run(common + ["--tbl=" + str(tbl), "--resident"], tmp_path)
+    generated = run(common, tmp_path)
+    for r in (cached, direct, generated):
+        assert r.returncode == 0, r.stderr
+    ref = tables(generated.stdout)
+    assert ref and ref[0]
+    assert tables(made.stdout) == ref and tables(parsed.stdout) == ref
+    assert tables(cached.stdout) == ref and tables(direct.stdout) == ref

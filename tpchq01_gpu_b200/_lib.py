@@ -222,6 +222,15 @@ SIGNATURES = {
     "q1_cache_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ColumnsOut)]),
     "q1_cache_load": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_uint64)]),
+    "q1_tbl_count_device": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), vp]),
+    "q1_tbl_parse_device": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.POINTER(ColumnsOut), ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_uint64), vp]),
+    "q1_tbl_read_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ColumnsOut), ctypes.c_uint64,
+                                        ctypes.POINTER(ctypes.c_uint64)]),
+    "q1_tbl_load": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_uint64)]),
+    "q1_tbl_format": (ctypes.c_int, [ctypes.POINTER(Columns), ctypes.c_uint64, ctypes.c_uint64, vp, ctypes.c_uint64,
+                                     ctypes.POINTER(ctypes.c_uint64)]),
     "q1_inject_fault": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32]),
     "q1_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_uint32, vp]),
     "q1_version": (ctypes.c_char_p, []),

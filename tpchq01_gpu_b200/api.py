@@ -9,6 +9,7 @@ Invalid combinations raise Q1Error with the reference's messages.
 Numbers are exact: every sum is a Python int (decoded from 128-bit two's complement).
 """
 import ctypes
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -154,6 +155,13 @@ class Q1Context:
         check(lib().q1_generate_table(self._h, seed, first_row, rows, LAYOUTS[layout], PACKINGS[packing],
                                       RESIDENCIES[residency]))
 
+    def load_tbl(self, path, layout="compressed", packing="pair", residency="hbm"):
+        """A lineitem .tbl file, parsed on the GPU; returns the row count."""
+        n = ctypes.c_uint64(0)
+        check(lib().q1_tbl_load(self._h, os.fsencode(path), LAYOUTS[layout], PACKINGS[packing],
+                                RESIDENCIES[residency], ctypes.byref(n)))
+        return n.value
+
     def run(self, params=None, **kw):
         params = params or Q1Params(**kw)
         p = params.to_c()
@@ -233,6 +241,34 @@ def generate_host(seed, first_row, rows):
     c = _lib.Columns(_ptr(cols["shipdate"]), _ptr(cols["discount"]), _ptr(cols["extendedprice"]), _ptr(cols["tax"]),
                      _ptr(cols["quantity"]), _ptr(cols["returnflag"]), _ptr(cols["linestatus"]))
     check(lib().q1_generate_host(seed, first_row, rows, ctypes.byref(c)))
+    return cols
+
+
+def tbl_format(cols, first_row=0):
+    """Reference-typed host columns as lineitem .tbl text (bytes)."""
+    n = len(cols["shipdate"])
+    c = _lib.Columns(_ptr(cols["shipdate"]), _ptr(cols["discount"]), _ptr(cols["extendedprice"]), _ptr(cols["tax"]),
+                     _ptr(cols["quantity"]), _ptr(cols["returnflag"]), _ptr(cols["linestatus"]))
+    size = ctypes.c_uint64(0)
+    check(lib().q1_tbl_format(ctypes.byref(c), first_row, n, None, 0, ctypes.byref(size)))
+    buf = np.empty(max(size.value, 1), np.uint8)
+    check(lib().q1_tbl_format(ctypes.byref(c), first_row, n, _ptr(buf), size.value, ctypes.byref(size)))
+    return buf[: size.value].tobytes()
+
+
+def tbl_read_file(path):
+    """Reference-typed host columns of a .tbl file, parsed on the current GPU."""
+    n = ctypes.c_uint64(0)
+    check(lib().q1_tbl_read_file(os.fsencode(path), None, 0, ctypes.byref(n)))
+    rows = n.value
+    cols = {
+        "shipdate": np.empty(rows, np.int32), "discount": np.empty(rows, np.int64),
+        "extendedprice": np.empty(rows, np.int64), "tax": np.empty(rows, np.int64),
+        "quantity": np.empty(rows, np.int64), "returnflag": np.empty(rows, "S1"), "linestatus": np.empty(rows, "S1"),
+    }
+    o = _lib.ColumnsOut(_ptr(cols["shipdate"]), _ptr(cols["returnflag"]), _ptr(cols["linestatus"]),
+                        _ptr(cols["discount"]), _ptr(cols["tax"]), _ptr(cols["extendedprice"]), _ptr(cols["quantity"]))
+    check(lib().q1_tbl_read_file(os.fsencode(path), ctypes.byref(o), rows, ctypes.byref(n)))
     return cols
 
 

@@ -83,6 +83,15 @@ uint32_t groupkey_part_min_groups();
 cudaError_t launch_generate_keys(uint64_t seed, uint64_t first_row, uint64_t rows, uint32_t num_groups,
                                  const uint32_t* dev_cdf, uint32_t* dev_keys, cudaStream_t stream);
 
+// lineitem text parsing (tbl_kernels.cu). tile_lines: tbl_tiles(bytes) + 1 words; after
+// launch_tbl_count it holds the newlines before each 64 KB tile and, last, the total.
+uint64_t tbl_tiles(uint64_t bytes);
+cudaError_t launch_tbl_count(const char* text, uint64_t bytes, unsigned long long* tile_lines, cudaStream_t stream);
+// bad: [malformed lines, byte offset of the first] (caller sets 0 and ~0)
+cudaError_t launch_tbl_parse(const char* text, uint64_t bytes, const unsigned long long* tile_first,
+                             int32_t* ship, int64_t* qty, int64_t* price, int64_t* disc, int64_t* tax, char* rf,
+                             char* ls, uint64_t capacity, unsigned long long* bad, cudaStream_t stream);
+
 // Utility kernels (util_kernels.cu).
 struct GenCompressedOut {
     uint16_t* shipdate;

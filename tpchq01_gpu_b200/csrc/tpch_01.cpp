@@ -37,7 +37,7 @@ static void print_help(const char* argv0) {
                     "      or in-registers, local-mem, per-thread-shared-mem)\n");
     fprintf(stderr, "   --runs=[default:5]\n");
     fprintf(stderr, "   --sf=[default:1.0] | --scale-factor=   --rows=N\n");
-    fprintf(stderr, "   --data-dir=DIR | --cache-dir=DIR   --write-cache\n");
+    fprintf(stderr, "   --data-dir=DIR | --cache-dir=DIR   --write-cache   --tbl=FILE   --write-tbl\n");
     fprintf(stderr, "   --cpu-fraction=[default:0.5]\n");
     fprintf(stderr, "   --streams=[default:4]\n");
     fprintf(stderr, "   --threads-per-block=[multiple of 32]\n");
@@ -110,8 +110,8 @@ int main(int argc, char** argv) {
     double scale_factor = 1.0;
     uint64_t rows = 0;
     uint64_t seed = 20260101;
-    bool print = false, resident = false, write_cache = false;
-    std::string data_dir, cache_dir;
+    bool print = false, resident = false, write_cache = false, write_tbl = false;
+    std::string data_dir, cache_dir, tbl_path;
     for (int i = 1; i < argc; ++i) {
         std::string a(argv[i]);
         if (!starts(a, "--")) {
@@ -136,6 +136,8 @@ int main(int argc, char** argv) {
             else if (name == "data-dir") data_dir = val;
             else if (name == "cache-dir") cache_dir = val;
             else if (name == "write-cache") write_cache = true;
+            else if (name == "tbl") tbl_path = val;
+            else if (name == "write-tbl") write_tbl = true;
             else if (name == "scale-factor" || name == "sf") {
                 scale_factor = std::stod(val);
                 if (scale_factor < 0.001) {
@@ -182,29 +184,85 @@ int main(int argc, char** argv) {
     const q1_residency res = resident ? Q1_RESIDENCY_HBM : Q1_RESIDENCY_PINNED_HOST;
     const q1_layout layout = p.apply_compression ? Q1_LAYOUT_COMPRESSED : Q1_LAYOUT_UNCOMPRESSED;
     q1_status st;
-    if (!data_dir.empty() || !cache_dir.empty()) {
-        // the reference's column cache: <data dir>/<scale factor as std::to_string>/ (src/main.cu:405-409)
+    if (!tbl_path.empty()) {
+        // a lineitem text file, parsed on the GPU (lineitem::FromFile, cpu/tpch_kit.cpp:155-172)
+        printf("Parsing the lineitem table in file %s on the GPU... ", tbl_path.c_str());
+        fflush(stdout);
+        st = q1_tbl_load(ctx, tbl_path.c_str(), layout, Q1_FLAGS_PAIR_2BIT, res, &rows);
+    } else if (!data_dir.empty() || !cache_dir.empty()) {
+        // the reference's column cache: <data dir>/<scale factor as std::to_string>/ (src/main.cu:405-409);
+        // without one, <dir>/lineitem.tbl is parsed and the cache written (src/main.cu:441-475)
         const std::string dir = !cache_dir.empty() ? cache_dir : data_dir + "/" + std::to_string(scale_factor);
+        const std::string tbl = dir + "/lineitem.tbl";
         uint64_t cached = 0;
         if (q1_cache_rows(dir.c_str(), &cached) != Q1_OK) {
-            if (!write_cache) {
-                fprintf(stderr, "%s (use --write-cache to generate one)\n", q1_last_error());
+            struct stat sb;
+            const bool have_tbl = stat(tbl.c_str(), &sb) == 0;
+            if (!have_tbl && !write_cache && !write_tbl) {
+                fprintf(stderr, "%s and no %s (use --write-cache or --write-tbl to generate one)\n", q1_last_error(),
+                        tbl.c_str());
                 q1_close(ctx);
                 return EXIT_FAILURE;
             }
-            printf("Writing a column cache of %llu generated rows to %s... ", (unsigned long long)rows, dir.c_str());
-            fflush(stdout);
             if (!data_dir.empty()) mkdir(data_dir.c_str(), 0755);
-            std::vector<int32_t> ship(rows);
-            std::vector<int64_t> disc(rows), price(rows), tax(rows), qty(rows);
-            std::vector<char> rf(rows), ls(rows);
+            mkdir(dir.c_str(), 0755);
+            std::vector<int32_t> ship;
+            std::vector<int64_t> disc, price, tax, qty;
+            std::vector<char> rf, ls;
+            auto resize = [&](uint64_t n) {
+                ship.resize(n), disc.resize(n), price.resize(n), tax.resize(n), qty.resize(n), rf.resize(n), ls.resize(n);
+            };
+            q1_status gs = Q1_OK;
+            if (have_tbl) {
+                printf("Parsing the lineitem table in file %s on the GPU... ", tbl.c_str());
+                fflush(stdout);
+                uint64_t n = 0;
+                gs = q1_tbl_read_file(tbl.c_str(), nullptr, 0, &n);
+                if (gs == Q1_OK) {
+                    resize(n);
+                    q1_columns_out o{ship.data(), rf.data(), ls.data(), disc.data(), tax.data(), price.data(), qty.data()};
+                    gs = q1_tbl_read_file(tbl.c_str(), &o, n, &rows);
+                }
+            } else {
+                resize(rows);
+                q1_columns c{ship.data(), disc.data(), price.data(), tax.data(), qty.data(), rf.data(), ls.data()};
+                gs = q1_generate_host(seed, 0, rows, &c);
+                if (gs == Q1_OK && write_tbl) {
+                    printf("Writing %llu generated rows to %s... ", (unsigned long long)rows, tbl.c_str());
+                    fflush(stdout);
+                    uint64_t bytes = 0;
+                    gs = q1_tbl_format(&c, 0, rows, nullptr, 0, &bytes);
+                    std::vector<char> text(gs == Q1_OK ? bytes : 0);
+                    if (gs == Q1_OK) gs = q1_tbl_format(&c, 0, rows, text.data(), bytes, &bytes);
+                    FILE* f = gs == Q1_OK ? fopen(tbl.c_str(), "wb") : nullptr;
+                    if (gs == Q1_OK && (!f || fwrite(text.data(), 1, bytes, f) != bytes)) {
+                        fprintf(stderr, "\ncannot write %s\n", tbl.c_str());
+                        if (f) fclose(f);
+                        q1_close(ctx);
+                        return EXIT_FAILURE;
+                    }
+                    if (f) fclose(f);
+                }
+            }
             q1_columns c{ship.data(), disc.data(), price.data(), tax.data(), qty.data(), rf.data(), ls.data()};
-            if (q1_generate_host(seed, 0, rows, &c) != Q1_OK || q1_cache_write(dir.c_str(), &c, rows) != Q1_OK) {
+            if (gs == Q1_OK && (have_tbl || write_cache)) {
+                printf("done (%llu rows).\nWriting the column cache to %s... ", (unsigned long long)rows, dir.c_str());
+                fflush(stdout);
+                gs = q1_cache_write(dir.c_str(), &c, rows);
+            }
+            if (gs != Q1_OK) {
                 fprintf(stderr, "\n%s\n", q1_last_error());
                 q1_close(ctx);
                 return EXIT_FAILURE;
             }
             printf("done.\n");
+            if (!have_tbl && !write_cache) {
+                // --write-tbl alone: load the generated rows directly
+                printf("Loading %llu rows... ", (unsigned long long)rows);
+                fflush(stdout);
+                st = q1_load_columns(ctx, &c, rows, layout, Q1_FLAGS_PAIR_2BIT, res);
+                goto loaded;
+            }
         }
         printf("Loading the column cache in %s... ", dir.c_str());
         fflush(stdout);
@@ -216,6 +274,7 @@ int main(int argc, char** argv) {
         fflush(stdout);
         st = q1_generate_table(ctx, seed, 0, rows, layout, Q1_FLAGS_PAIR_2BIT, res);
     }
+loaded:
     if (st != Q1_OK) {
         fprintf(stderr, "\nloading the table failed: %s\n", q1_last_error());
         q1_close(ctx);
