@@ -22,8 +22,22 @@ namespace {
 
 struct DeviceMem {
     void* p = nullptr;
+    cudaStream_t st = nullptr;   // set: stream-ordered allocation (no device-wide sync on free)
     ~DeviceMem() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (st) cudaFreeAsync(p, st);
+            else cudaFree(p);
+        }
+    }
+    q1_status alloc_async(uint64_t bytes, cudaStream_t stream) {
+        if (take_fault(kFaultDeviceAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected device allocation failure");
+        if (cudaMallocAsync(&p, bytes ? bytes : 16, stream) != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return set_error(Q1_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
+        }
+        st = stream;
+        return Q1_OK;
     }
     q1_status alloc(uint64_t bytes) {
         if (take_fault(kFaultDeviceAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected device allocation failure");
@@ -146,7 +160,7 @@ q1_status q1_tbl_count_device(const char* dev_text, uint64_t bytes, uint64_t* ro
     cudaStream_t st = (cudaStream_t)cuda_stream;
     const uint64_t tiles = tbl_tiles(bytes);
     DeviceMem lines;
-    q1_status s = lines.alloc((tiles + 1) * 8);
+    q1_status s = lines.alloc_async((tiles + 1) * 8, st);
     if (s != Q1_OK) return s;
     auto* v = static_cast<unsigned long long*>(lines.p);
     Q1_CUDA(launch_tbl_count(dev_text, bytes, v, st));
@@ -174,7 +188,7 @@ q1_status q1_tbl_parse_device(const char* dev_text, uint64_t bytes, const q1_col
     cudaStream_t st = (cudaStream_t)cuda_stream;
     const uint64_t tiles = tbl_tiles(bytes);
     DeviceMem scratch;
-    q1_status s = scratch.alloc((tiles + 3) * 8);
+    q1_status s = scratch.alloc_async((tiles + 3) * 8, st);
     if (s != Q1_OK) return s;
     auto* v = static_cast<unsigned long long*>(scratch.p);
     unsigned long long* bad = v + tiles + 1;

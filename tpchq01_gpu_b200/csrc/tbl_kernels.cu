@@ -17,9 +17,10 @@
 // Kernels (64 KB text tiles, 256 threads, 256 bytes a thread):
 //   tbl_count_kernel  newlines per tile (16-byte loads, byte compares on 32-bit words)
 //   tbl_scan_kernel   exclusive prefix of the tile counts (one CTA)
-//   tbl_parse_kernel  recounts its tile, ranks each thread's newlines with a block scan, and
-//                     parses every line that starts after one of them (row = newlines before
-//                     it); thread 0 of tile 0 also parses the line at byte 0.
+//   tbl_parse_kernel  recounts its tile, ranks each thread's newlines with a block scan,
+//                     gathers the line starts into shared memory in text order and parses them
+//                     lane-parallel (row = newlines before the line); thread 0 of tile 0 also
+//                     parses the line at byte 0.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -52,20 +53,40 @@ __device__ __forceinline__ uint32_t count_newlines(const char* __restrict__ text
 
 // Day number of a civil date counted the MonetDB way (days since a year 0, years >= 1 here);
 // -1 for a date that does not exist.
+__device__ __forceinline__ int32_t days_before_month(int32_t m) {   // non-leap year, m in 1..13
+    return (367 * m - 362) / 12 - (m > 2 ? 2 : 0);
+}
 __device__ __forceinline__ int32_t day_number(int32_t y, int32_t m, int32_t d) {
     const bool leap = (y % 4 == 0) && (y % 100 != 0 || y % 400 == 0);
-    const int32_t mdays[13] = {0, 31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
-    const int32_t before[13] = {0, 0, 31, 59, 90, 120, 151, 181, 212, 243, 273, 304, 334};
     if (y < 1 || y > 999999 || m < 1 || m > 12 || d < 1) return -1;
-    if (d > mdays[m] + ((m == 2 && leap) ? 1 : 0)) return -1;
+    const int32_t len = (m == 12 ? 31 : days_before_month(m + 1) - days_before_month(m)) + ((m == 2 && leap) ? 1 : 0);
+    if (d > len) return -1;
     const int32_t p = y - 1;
-    return 365 * y + (p / 4 - p / 100 + p / 400 + 1) + before[m] + ((m > 2 && leap) ? 1 : 0) + d - 1;
+    return 365 * y + (p / 4 - p / 100 + p / 400 + 1) + days_before_month(m) + ((m > 2 && leap) ? 1 : 0) + d - 1;
 }
 
+// Reads a line through a 16-byte window: one aligned 16-byte load per 16 bytes of the line
+// (lanes of a warp read different lines, so every load touches a different cache line; byte
+// loads would cost one L1 wavefront per byte). The last, partial 16-byte block of the buffer is
+// read bytewise so that no load goes past its end.
 struct Cursor {
     const char* __restrict__ t;
     uint64_t p, end;
-    __device__ __forceinline__ int peek() const { return p < end ? (int)(unsigned char)t[p] : -1; }
+    uint64_t wbase = ~0ull;   // window: bytes [wbase, wbase + 16) of the address space
+    uint4 win;
+    __device__ __forceinline__ int peek() {
+        if (p >= end) return -1;
+        const uint64_t addr = reinterpret_cast<uint64_t>(t) + p;
+        const uint64_t base = addr & ~15ull;
+        if (base + 16 > reinterpret_cast<uint64_t>(t) + end) return (int)(unsigned char)t[p];
+        if (base != wbase) {
+            win = __ldg(reinterpret_cast<const uint4*>(base));
+            wbase = base;
+        }
+        const uint32_t o = (uint32_t)(addr & 15u);
+        const uint32_t w = o < 8 ? (o < 4 ? win.x : win.y) : (o < 12 ? win.z : win.w);
+        return (int)((w >> (8 * (o & 3u))) & 0xFFu);
+    }
     // skips to just after the next '|' of this line; false at '\n' or the end
     __device__ __forceinline__ bool skip_field() {
         for (;;) {
@@ -205,14 +226,22 @@ __global__ void __launch_bounds__(1024) tbl_scan_kernel(unsigned long long* v, u
     if (threadIdx.x == 0) v[tiles] = carry;
 }
 
+// Parses the lines that start in this block's tile. The line starts are first gathered into
+// shared memory in text order (each thread's newlines at its block-scan rank), then every thread
+// parses lines tid, tid + 256, ...: the lanes of a warp parse different lines side by side instead
+// of one lane at a time. Tiles with more than kList lines take several rounds.
 __global__ void __launch_bounds__(tbl::kThreads) tbl_parse_kernel(const char* __restrict__ text, uint64_t bytes,
                                                                   const unsigned long long* __restrict__ tile_first,
                                                                   tbl::Out o, uint64_t capacity,
                                                                   unsigned long long* __restrict__ bad) {
     using namespace tbl;
+    constexpr uint32_t kList = 4096;
     __shared__ uint32_t warp_sum[kThreads / 32];
+    __shared__ uint32_t total;
+    __shared__ uint32_t starts[kList];   // newline offsets within the tile, in text order
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint64_t a = blockIdx.x * kTile + (uint64_t)tid * kPerThread;
+    const uint64_t tile = blockIdx.x * kTile;
+    const uint64_t a = tile + (uint64_t)tid * kPerThread;
     const uint64_t b = a + kPerThread < bytes ? a + kPerThread : bytes;
     const uint32_t n = a < bytes ? count_newlines(text, a, b) : 0u;
     // block-wide exclusive prefix of n
@@ -226,24 +255,55 @@ __global__ void __launch_bounds__(tbl::kThreads) tbl_parse_kernel(const char* __
     __syncthreads();
     uint32_t before = 0;
     for (uint32_t w = 0; w < warp; ++w) before += warp_sum[w];
-    uint64_t k = tile_first[blockIdx.x] + before + (inc - n);   // newlines before this thread's bytes
+    before += inc - n;
+    if (tid == kThreads - 1) total = before + n;
+    __syncthreads();
+    const uint32_t T = total;
+    const unsigned long long first = tile_first[blockIdx.x];   // newlines before this tile
     unsigned long long nbad = 0, first_bad = ~0ull;
-    if (blockIdx.x == 0 && tid == 0 && bytes > 0 && capacity > 0) {
-        if (!parse_line(text, bytes, 0, 0, o)) ++nbad, first_bad = 0;
-    }
-    for (uint64_t i = a; i < b && n; ++i) {
-        if (text[i] != '\n') continue;
-        ++k;                                  // the line after this newline is row k
-        if (i + 1 >= bytes) break;            // a final '\n' starts no row
-        if (k >= capacity) {
+    auto one = [&](uint64_t s, uint64_t row) {
+        if (row >= capacity || !parse_line(text, bytes, s, row, o)) {
             ++nbad;
-            if (i + 1 < first_bad) first_bad = i + 1;
-            continue;
+            if (s < first_bad) first_bad = s;
         }
-        if (!parse_line(text, bytes, i + 1, k, o)) {
-            ++nbad;
-            if (i + 1 < first_bad) first_bad = i + 1;
+    };
+    if (blockIdx.x == 0 && tid == 0 && bytes > 0) one(0, 0);
+    const bool vec = b - a == kPerThread && ((reinterpret_cast<uintptr_t>(text) + a) & 15u) == 0;
+    for (uint32_t r0 = 0; r0 < T; r0 += kList) {
+        // gather: this thread's newlines whose block rank falls in [r0, r0 + kList)
+        if (n && before + n > r0 && before < r0 + kList) {
+            uint32_t k = before;
+            if (vec) {
+                const uint4* p = reinterpret_cast<const uint4*>(text + a);
+                for (uint32_t q = 0; q < kPerThread / 16; ++q) {
+                    const uint4 v = __ldg(p + q);
+                    const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (uint32_t h = 0; h < 4; ++h) {
+                        uint32_t m = __vcmpeq4(w4[h], 0x0A0A0A0Au) & 0x80808080u;
+                        while (m) {
+                            const uint32_t byte = (uint32_t)(__ffs(m) - 1) >> 3;
+                            m &= m - 1;
+                            if (k >= r0 && k < r0 + kList) starts[k - r0] = (uint32_t)(a - tile) + q * 16 + h * 4 + byte;
+                            ++k;
+                        }
+                    }
+                }
+            } else {
+                for (uint64_t i = a; i < b; ++i) {
+                    if (text[i] != '\n') continue;
+                    if (k >= r0 && k < r0 + kList) starts[k - r0] = (uint32_t)(i - tile);
+                    ++k;
+                }
+            }
         }
+        __syncthreads();
+        const uint32_t cnt = T - r0 < kList ? T - r0 : kList;
+        for (uint32_t j = tid; j < cnt; j += kThreads) {
+            const uint64_t i = tile + starts[j];            // a newline; the next line is row first + rank + 1
+            if (i + 1 < bytes) one(i + 1, first + r0 + j + 1);
+        }
+        __syncthreads();
     }
     if (nbad) {
         atomicAdd(&bad[0], nbad);
