@@ -166,6 +166,33 @@ def run_reference_cpu(rows, seconds=None, steps=None, warmup=0, threads=None):
     return rows * len(times) / sum(times), used, times
 
 
+def reference_comparators(rows=20_000_000, reps=3):
+    """The reference's single-thread tuple-at-a-time kernels as extra CPU comparators (rows/s,
+    best of `reps`): KernelHyPer<true> on the int64 columns and KernelHyPerCompact<true> on the
+    compact int8/int16/int32 copy. The reference's AVX-512 kernel (cpu/kernel_avx512.hpp) is
+    disabled in the reference (cpu/q1.cpp:14-15) and gathers/scatters through the addresses of
+    its table pointers ((int64_t*)&aggr_avx0_count, :178-184) instead of the tables, so it is not
+    run."""
+    from oracle import py_oracle as O
+    import tpchq01_gpu_b200 as q
+    cols = q.generate_host(SEED, 0, rows)
+    out = {}
+    for name, shift, fn in [("hyper_1_thread", 0, "hyper"), ("hyper_compact_1_thread", O.HYPER_COMPACT_SHIFT,
+                                                             "hyper_compact")]:
+        t = O.RefTable(cols, CUTOFF - shift)
+        try:
+            best = None
+            for _ in range(reps):
+                s = time.perf_counter()
+                _, flag = getattr(t, fn)()
+                el = time.perf_counter() - s
+                best = el if best is None else min(best, el)
+            out[name] = {"rows_per_s": rows / best, "rows": rows, "overflow": bool(flag)}
+        finally:
+            t.close()
+    return out
+
+
 def reference_gpu_arm(args):
     """The reference's own compressed GPU kernels (src/kernels/*, built unmodified for sm_100a
     into oracle/_ref/libq1refgpu.so) on the same B200, HBM-resident separate-flags layout
@@ -254,6 +281,10 @@ def reference_arm(args, rank):
             "data": "synthetic", "config": config_dict(args.gpus, args.placement),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["comparators"] = reference_comparators()
+    except Exception as e:   # informative only
+        line["comparators"] = {"unavailable": str(e)}
     print(json.dumps(line), flush=True)
     return 0
 

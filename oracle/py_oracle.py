@@ -138,6 +138,12 @@ def precompute_filter(c_shipdate, cutoff_day):
     return out
 
 
+# KernelHyPerCompact compares the compact ship date (ship - 727563 under -DGPU) with the int16
+# truncation of the cutoff day (729999 -> 9103): pushing the table with cutoff_day - 6667 makes it
+# evaluate ship <= cutoff_day.
+HYPER_COMPACT_SHIFT = 6667
+
+
 class RefTable:
     """The reference's lineitem (cpu/tpch_kit.hpp:135-149) filled through Column::Push."""
 
@@ -155,6 +161,15 @@ class RefTable:
     def hyper(self):
         buf = np.zeros(NG * NA * 2, dtype=np.uint64)
         flag = ref().q1ref_hyper(self.h, ptr(buf))
+        return i128_to_ints(buf, NG), flag
+
+    def hyper_compact(self):
+        """KernelHyPerCompact<true>; the table must have been pushed with HYPER_COMPACT_SHIFT
+        subtracted from the cutoff day (see q1ref_hyper_compact)."""
+        r = ref()
+        r.q1ref_hyper_compact.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+        flag = r.q1ref_hyper_compact(self.h, ptr(buf))
         return i128_to_ints(buf, NG), flag
 
     def x100(self, offset=0, num=None):

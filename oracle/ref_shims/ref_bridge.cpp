@@ -5,6 +5,7 @@
 //
 // Kernels exposed:
 //   KernelHyPer<true>                    cpu/kernel_hyper.hpp:6-96 (tuple at a time, int128 sums)
+//   KernelHyPerCompact<true>             cpu/kernel_hyper_compact.hpp (same loop, compact columns)
 //   lineitem text values                 Decimal<15,2> / Char / Date (cpu/tpch_kit.hpp, .cpp)
 //   KernelX100<kMagic,true,kNoAvx512>    cpu/kernel_x100.hpp:16-405 (vectorised, partial shuffle)
 // The reference's own multi-threaded driver, Morsel<> (cpu/kernel_x100.hpp:423-665), returns
@@ -26,6 +27,7 @@
 
 #include "common.hpp"
 #include "kernel_hyper.hpp"
+#include "kernel_hyper_compact.hpp"
 #include "vectorized.hpp"
 #include "kernel_x100.hpp"
 
@@ -179,6 +181,22 @@ int q1ref_hyper(void* t, i128* out) {
     RefTable* r = (RefTable*)t;
     g_overflow.store(0);
     KernelHyPer<true> k(r->li);
+    k.Clear();
+    k();
+    table_to_groups_hyper(k.aggrs0, out);
+    return g_overflow.load();
+}
+
+// KernelHyPerCompact<true> (cpu/kernel_hyper_compact.hpp): HyPer's tuple-at-a-time loop over the
+// int8/int16/int32 compact copy (ComprData, cpu/common.cpp:113-137). Built with -DGPU (as the
+// reference's GPU binary is), the compact ship date is ship - 727563 while this kernel compares it
+// with the int16 truncation of the cutoff day (729999 -> 9103), so the table must be pushed with
+// cutoff_day - 6667 to evaluate Q1's predicate. out: [6][6] int128. Returns 1 on overflow.
+int q1ref_hyper_compact(void* t, i128* out) {
+    RefTable* r = (RefTable*)t;
+    use_compact_copy_of(r->li);
+    g_overflow.store(0);
+    KernelHyPerCompact<true> k(r->li, 0);
     k.Clear();
     k();
     table_to_groups_hyper(k.aggrs0, out);

@@ -33,3 +33,16 @@ def test_x100_partial_ranges_add_up():
     whole, _ = t.x100()
     t.close()
     assert np.array_equal(a + b, whole)
+
+
+@pytest.mark.parametrize("seed,rows,cutoff", [(106, 120_000, 729999), (107, 33_333, 729906), (108, 50_000, 727600)])
+def test_hyper_compact_equals_restatement(seed, rows, cutoff):
+    """The reference's KernelHyPerCompact (compact int8/int16/int32 columns) gives the same tables,
+    with the ship-date shift its int16 cutoff needs under the GPU build."""
+    cols = gen_np.generate(seed, 0, rows)
+    mine, _ = O.q1_uncompressed(cols, cutoff)
+    t = O.RefTable(cols, cutoff - O.HYPER_COMPACT_SHIFT)
+    compact, flag = t.hyper_compact()
+    t.close()
+    assert flag == 0
+    assert np.array_equal(mine, compact)
