@@ -39,6 +39,7 @@ __device__ __forceinline__ void byte_planes(const uint32_t w[4], uint32_t out[4]
 //   sum (100-d)(100+t) p  sum_k 2^8k (dp4a(ABL & M, P_k) + 2^8 dp4a(ABH & M, P_k))
 // Every 32-bit partial stays exact while a thread adds at most 2^15 rows per launch (the host
 // caps launches accordingly): the largest, an ab-low plane, grows by <= 4*255*255 per quad.
+// A quad whose four prices are below 2^24 has a zero top plane and may skip its 4 dp4a.
 struct GroupPlanes {
     uint32_t cnt, q, d;
     uint32_t p[4], dp[4], chl[4], chh[4];
@@ -47,6 +48,9 @@ struct GroupPlanes {
 #pragma unroll
         for (int k = 0; k < 4; ++k) p[k] = dp[k] = chl[k] = chh[k] = 0;
     }
+    // kTop: the prices' top byte plane may be nonzero. Callers pass false when no lane of the
+    // warp has a price >= 2^24 in the quad (TPC-H prices stay below 2^24): 15 dp4a instead of 19.
+    template <bool kTop = true>
     __device__ __forceinline__ void add_quad(uint32_t OH, uint32_t g, const Quad& x) {
         const uint32_t W1 = (OH >> g) & 0x01010101u;
         const uint32_t M = (W1 << 8) - W1;   // 0xFF in the group's row bytes
@@ -55,7 +59,7 @@ struct GroupPlanes {
         q = __dp4a(W1, x.Q, q);
         d = __dp4a(W1, x.D, d);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < (kTop ? 4 : 3); ++k) {
             p[k] = __dp4a(W1, x.P[k], p[k]);
             dp[k] = __dp4a(MA, x.P[k], dp[k]);
             chl[k] = __dp4a(ML, x.P[k], chl[k]);

@@ -245,21 +245,27 @@ struct AccPerThread {
     // Called by all lanes of the warp. With the six (returnflag, linestatus) groups of the separate
     // flag layout, A/O and R/O (groups 1 and 5) need a receipt date before the ship date and do
     // not occur in TPC-H data: their planes run only when a lane of the warp has such a row.
+    template <bool kTop>
+    __device__ __forceinline__ void add_quad_planes(const Quad& x) {
+        if constexpr (G == 6) {
+            gq[0].template add_quad<kTop>(x.OH, 0u, x);
+            gq[2].template add_quad<kTop>(x.OH, 2u, x);
+            gq[3].template add_quad<kTop>(x.OH, 3u, x);
+            gq[4].template add_quad<kTop>(x.OH, 4u, x);
+            if (__any_sync(0xffffffffu, x.OH & 0x22222222u)) {
+                gq[1].template add_quad<kTop>(x.OH, 1u, x);
+                gq[5].template add_quad<kTop>(x.OH, 5u, x);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < G; ++i) gq[i].template add_quad<kTop>(x.OH, (uint32_t)i, x);
+        }
+    }
     __device__ __forceinline__ void add_quad(const Quad& x) {
         if constexpr (!kWideQty) {
-            if constexpr (G == 6) {
-                gq[0].add_quad(x.OH, 0u, x);
-                gq[2].add_quad(x.OH, 2u, x);
-                gq[3].add_quad(x.OH, 3u, x);
-                gq[4].add_quad(x.OH, 4u, x);
-                if (__any_sync(0xffffffffu, x.OH & 0x22222222u)) {
-                    gq[1].add_quad(x.OH, 1u, x);
-                    gq[5].add_quad(x.OH, 5u, x);
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < G; ++i) gq[i].add_quad(x.OH, (uint32_t)i, x);
-            }
+            // the prices' top byte plane is zero for the whole warp unless a price is >= 2^24
+            if (__any_sync(0xffffffffu, x.P[3])) add_quad_planes<true>(x);
+            else add_quad_planes<false>(x);
         }
     }
     __device__ __forceinline__ void fold() {
