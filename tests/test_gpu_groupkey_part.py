@@ -1,9 +1,10 @@
-"""The high-cardinality paths of the group-key shared placement against the oracle. Up to 4096
-groups one pass keeps a shared slot per group (3-stage ring above 2048); above that the library
-chooses on the device, from a sample of the rows, between that single pass (keys < 4096 in
-slots, larger keys into global accumulators) and a two-pass radix partition (rows partitioned by
-key into 8-byte records, then one shared-memory slot table per 4096-key partition).
-Q1_GROUPKEY_PATH forces either path so that both are checked: group counts on both sides of the
+"""The high-cardinality paths of the group-key shared placement against the oracle. Above 256
+groups the library chooses on the device, from a sample of the rows, among: one pass with a
+shared slot per key < 4096 (3-stage ring above 2048 groups; larger keys into global
+accumulators), every passing row straight into global accumulators (few passing rows over spread
+keys), and, above 4096 groups, a two-pass radix partition (rows partitioned by key into 8-byte
+records, then one shared-memory slot table per 4096-key partition). Q1_GROUPKEY_PATH forces each
+path so that all are checked: group counts on both sides of the
 partition width, uniform and Zipf keys, cutoffs from nothing to everything passing, ragged and
 tiny row counts, few-CTA launches (partition changes and table flushes inside a CTA) and a
 launch that crosses the 2^27-row segment boundary (against the global placement and the row
@@ -25,7 +26,7 @@ ROWS = 400_037
 SEED = 555
 
 
-PATHS = ["partitioned", "single", "auto"]
+PATHS = ["partitioned", "single", "global", "auto"]
 
 
 @pytest.fixture(scope="module")
@@ -44,9 +45,10 @@ def path(request, monkeypatch):
     return request.param
 
 
-@pytest.mark.parametrize("num_groups", [2049, 3000, 4096])
+@pytest.mark.parametrize("num_groups", [257, 2049, 3000, 4096])
 @pytest.mark.parametrize("dist", ["uniform", "zipf"])
-def test_wide_slots_match_oracle(table, num_groups, dist):
+@pytest.mark.parametrize("path", ["single", "global", "auto"], indirect=True)
+def test_wide_slots_match_oracle(table, path, num_groups, dist):
     comp, c, _ = table
     keys, _ = keys_for(num_groups, dist)
     for cutoff in [727000, 727600, 729999, 730089]:

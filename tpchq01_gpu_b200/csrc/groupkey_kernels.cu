@@ -13,11 +13,12 @@
 //   shared_mem_per_thread    num_groups <= 64: shared (group, discount, tax) cells
 //                            (Cube3Table); <= 256: shared (group, discount) cells (CubeTable);
 //                            <= 4096: shared per-group slots (SlotTable, 3-stage ring above
-//                            2048 groups); above that either this kernel with keys < 4096 in
+//                            2048 groups), or, above 4096, this kernel with keys < 4096 in
 //                            slots and larger keys reduced straight into the global
 //                            accumulators, or the two-pass partitioned path of
-//                            groupkey_part.cu, chosen on the device from a sample of the rows
-//                            (q1_groupkey_choose)
+//                            groupkey_part.cu; above 256 groups the path (and the global
+//                            placement's, when few rows pass over spread keys) is chosen on the
+//                            device from a sample of the rows (q1_groupkey_choose)
 //   global                   every passing row reduces into the global accumulators
 //
 // Accumulators live in scratch memory (per launch, zeroed first): per group 8 x u64 (see
@@ -269,46 +270,72 @@ static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_bl
 }
 
 static uint64_t acc_bytes(uint32_t num_groups) { return 64ull * num_groups; }
-static bool two_paths(int placement, uint32_t num_groups) {
-    return placement == kPlaceSharedMemPerThread && num_groups >= groupkey_part_min_groups();
+// The shared placement chooses its path on the device above 256 groups (the slot-table sizes).
+static bool chosen_on_device(int placement, uint32_t num_groups) {
+    return placement == kPlaceSharedMemPerThread && num_groups > ka::kCubeMaxGroups;
 }
 
-// For more than 4096 groups in the shared placement, picks one of two exact paths from 8192
-// evenly spaced sample rows and writes it to *mode:
+// Chooses the path of the shared placement for more than 256 groups from 8192 evenly spaced
+// sample rows and writes it to *mode (every path gives identical results):
+//   kModeGlobalPath   every passing row straight into the global accumulators, when fewer than
+//                     2% of the rows pass and no key occurs more than 3 times among the sampled
+//                     passing rows (global atomics on spread keys do not contend: 1.29 ms per
+//                     600 M rows at 1% pass, against 2.0 ms for the slot table; frequent keys make
+//                     them contend, 11.7 ms for Zipf keys at 1% pass);
 //   kModeSinglePass   the group-key kernel: keys < 4096 in a shared slot table, passing rows of
 //                     larger ("cold") keys straight into the global accumulators;
-//   kModePartitioned  the two-pass radix partition (groupkey_part.cu).
-// Cost model fitted to both paths on a B200 (ms per 600 M rows; c = fraction of the rows that
-// pass with a cold key, p = fraction that pass): single pass 2.2 + 20 c + 0.3 p; partitioned
-// 1.7 + 4.3 c + 5.65 (p - c), the hot rows costing more there because skewed keys contend for
-// the same ring counters and slots. The single pass wins when 21.35 c - 5.35 p < -0.5: skewed
-// keys with many passing rows. Both paths give identical results.
+//   kModePartitioned  (more than 4096 groups) the two-pass radix partition (groupkey_part.cu).
+// Between the last two, a cost model fitted to both paths on a B200 (ms per 600 M rows; c =
+// fraction of the rows that pass with a cold key, p = fraction that pass): single pass 2.2 + 20 c
+// + 0.3 p; partitioned 1.7 + 4.3 c + 5.65 (p - c), the hot rows costing more there because skewed
+// keys contend for the same ring counters and slots. The single pass wins when
+// 21.35 c - 5.35 p < -0.5: skewed keys with many passing rows.
 __global__ void __launch_bounds__(256) q1_groupkey_choose(const uint16_t* __restrict__ ship,
                                                           const uint32_t* __restrict__ keys, uint64_t rows,
-                                                          int32_t cutoff, uint32_t hot, uint32_t force,
-                                                          uint32_t* mode) {
-    constexpr uint32_t K = 8192;
+                                                          int32_t cutoff, uint32_t hot, uint32_t allow_part,
+                                                          uint32_t force, uint32_t* mode) {
+    constexpr uint32_t K = 8192, kList = 512;
     if (force) {
         if (threadIdx.x == 0) *mode = force;
         return;
     }
-    __shared__ uint32_t cnt[2];
-    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    __shared__ uint32_t cnt[4];       // passing, cold, listed, largest key multiplicity
+    __shared__ uint32_t list[kList];  // keys of the sampled passing rows
+    if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
     __syncthreads();
     uint32_t pass = 0, cold = 0;
     for (uint32_t j = threadIdx.x; j < K; j += blockDim.x) {
         const uint64_t i = (uint64_t)j * rows / K;
         if ((int32_t)ship[i] <= cutoff) {
+            const uint32_t key = keys[i];
             ++pass;
-            cold += keys[i] >= hot ? 1u : 0u;
+            cold += key >= hot ? 1u : 0u;
+            const uint32_t at = atomicAdd(&cnt[2], 1u);
+            if (at < kList) list[at] = key;
         }
     }
     atomicAdd(&cnt[0], pass);
     atomicAdd(&cnt[1], cold);
     __syncthreads();
+    const uint32_t P = cnt[0], C = cnt[1], L = cnt[2] < kList ? cnt[2] : kList;
+    const bool few = (uint64_t)P * 50 < K && cnt[2] <= kList;
+    if (few) {
+        for (uint32_t e = threadIdx.x; e < L; e += blockDim.x) {
+            uint32_t m = 0;
+            for (uint32_t x = 0; x < L; ++x) m += list[x] == list[e] ? 1u : 0u;
+            atomicMax(&cnt[3], m);
+        }
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        const int64_t score = 2135ll * cnt[1] - 535ll * cnt[0];   // 100 x (21.35 c - 5.35 p) x K
-        *mode = score < -50ll * K ? kModeSinglePass : kModePartitioned;
+        if (few && cnt[3] <= 3) {
+            *mode = kModeGlobalPath;
+        } else if (!allow_part) {
+            *mode = kModeSinglePass;
+        } else {
+            const int64_t score = 2135ll * C - 535ll * P;   // 100 x (21.35 c - 5.35 p) x K
+            *mode = score < -50ll * K ? kModeSinglePass : kModePartitioned;
+        }
     }
 }
 
@@ -318,14 +345,15 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
     cudaError_t e = cudaMemsetAsync(scratch, 0, acc_bytes(num_groups), stream);
     if (e != cudaSuccess) return e;
     uint8_t* workspace = reinterpret_cast<uint8_t*>(scratch) + ((acc_bytes(num_groups) + 255) & ~255ull);
-    uint32_t* mode = two_paths(placement, num_groups)
-                         ? reinterpret_cast<uint32_t*>(workspace + groupkey_part_mode_offset())
-                         : nullptr;
-    // Q1_GROUPKEY_PATH=single|partitioned overrides the sample-based choice (tests and tuning)
+    const bool choose = chosen_on_device(placement, num_groups);
+    const bool part = num_groups >= groupkey_part_min_groups();
+    uint32_t* mode = choose ? reinterpret_cast<uint32_t*>(workspace + groupkey_part_mode_offset()) : nullptr;
+    // Q1_GROUPKEY_PATH=single|partitioned|global overrides the sample-based choice (tests, tuning)
     uint32_t force = 0;
     if (const char* env = std::getenv("Q1_GROUPKEY_PATH")) {
         if (!std::strcmp(env, "single")) force = kModeSinglePass;
-        else if (!std::strcmp(env, "partitioned")) force = kModePartitioned;
+        else if (!std::strcmp(env, "partitioned") && part) force = kModePartitioned;
+        else if (!std::strcmp(env, "global")) force = kModeGlobalPath;
     }
     const uint64_t kMaxRows = 1ull << 31;
     for (uint64_t off = 0; off < rows; off += kMaxRows) {
@@ -343,10 +371,16 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
         if (mode) {
             q1_groupkey_choose<<<1, 256, 0, stream>>>(reinterpret_cast<const uint16_t*>(prm.col[0]),
                                                       reinterpret_cast<const uint32_t*>(prm.col[5]), n, cutoff_rel,
-                                                      gk::kWideSlots, force, mode);
+                                                      gk::kWideSlots, part ? 1u : 0u, force, mode);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             prm.mode = mode;
             prm.mode_want = kModeSinglePass;
+            // the global path of the choice (returns at once unless chosen)
+            GroupKeyParams g = prm;
+            g.table = gk::kTableNone;
+            g.stages = gk::kMaxStages;
+            g.mode_want = kModeGlobalPath;
+            if ((e = launch_gk<kPlaceGlobal, 4>(g, sm_count, max_blocks, stream)) != cudaSuccess) return e;
         }
         switch (placement) {
             case kPlaceInRegistersPerThread:
@@ -358,7 +392,7 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
             default: return cudaErrorInvalidValue;
         }
         if (e != cudaSuccess) return e;
-        if (mode) {
+        if (mode && part) {
             e = launch_groupkey_part(prm.col, n, cutoff_rel, num_groups, scratch, workspace, mode, status, sm_count,
                                      max_blocks, stream);
             if (e != cudaSuccess) return e;
@@ -375,12 +409,13 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
     return cudaSuccess;
 }
 
-// The accumulators; for more than 4096 groups (two paths of the shared placement) also the
-// partition workspace after them.
+// The accumulators; above 256 groups also the mode word of the shared placement's path choice,
+// and above 4096 groups the partition workspace (which holds that word).
 uint64_t groupkey_scratch_bytes(uint32_t num_groups) {
-    return num_groups >= groupkey_part_min_groups()
-               ? ((acc_bytes(num_groups) + 255) & ~255ull) + groupkey_part_workspace_bytes()
-               : acc_bytes(num_groups);
+    const uint64_t a = (acc_bytes(num_groups) + 255) & ~255ull;
+    if (num_groups >= groupkey_part_min_groups()) return a + groupkey_part_workspace_bytes();
+    if (num_groups > ka::kCubeMaxGroups) return a + 256;   // the path choice's mode word
+    return acc_bytes(num_groups);
 }
 
 // Group keys of the seeded generator: uniform over [0, G) (cdf == nullptr) or by inverse CDF.

@@ -70,7 +70,7 @@ uint64_t groupkey_scratch_bytes(uint32_t num_groups);
 // partition by key, then per-partition shared-memory slot tables. acc: num_groups x 8 u64
 // (zeroed by the caller); workspace: groupkey_part_workspace_bytes(), 256-byte aligned. When
 // `mode` is set, every kernel of the path returns at once unless *mode == kModePartitioned.
-enum GroupKeyMode : uint32_t { kModeSinglePass = 1, kModePartitioned = 2 };
+enum GroupKeyMode : uint32_t { kModeSinglePass = 1, kModePartitioned = 2, kModeGlobalPath = 3 };
 cudaError_t launch_groupkey_part(const uint8_t* const cols[6], uint64_t rows, int32_t cutoff_rel,
                                  uint32_t num_groups, unsigned long long* acc, uint8_t* workspace,
                                  const uint32_t* mode, uint32_t* status, int sm_count, int max_blocks,
