@@ -342,20 +342,23 @@ q1_status q1_sync_check(void* cuda_stream);
 /* reference's 6-entry group table (src/constants.hpp:56) to many groups.                      */
 /* ------------------------------------------------------------------------------------------ */
 
-/* Bytes of device scratch q1_launch_groupkey needs for num_groups groups: 64 per group, plus
- * about 1.1 GB of partition workspace above 2048 groups (independent of the row count). */
+/* Bytes of device scratch q1_launch_groupkey needs for num_groups groups: 64 per group, plus 256
+ * above 256 groups and about 1.1 GB of partition workspace above 4096 groups (independent of
+ * the row count). */
 uint64_t q1_groupkey_scratch_bytes(uint32_t num_groups);
 
 /* Placements: IN_REGISTERS_PER_THREAD (num_groups <= 8; per-thread byte-plane sums),
  * SHARED_MEM_PER_THREAD (per-CTA shared-memory tables: (group, discount, tax) cells for
- * num_groups <= 64, (group, discount) cells for <= 256, one slot per group for <= 2048; above
- * that the passing rows are first partitioned by key into 8-byte records, 2^27 rows at a time,
- * and each partition of 4096 keys is then aggregated in a shared-memory slot table),
- * GLOBAL (global atomics for every row). Reads ship, qty, disc, tax, price of dev_cols and dev_keys; the result
- * accumulates into dev_aggregates[num_groups][6] (caller-zeroed int128). dev_scratch: device
- * memory of q1_groupkey_scratch_bytes(num_groups), owned by the caller; calls on different
- * streams need different scratch. A key >= num_groups in a passing row is reported as
- * Q1_ERR_DOMAIN by q1_sync_check. */
+ * num_groups <= 64, (group, discount) cells for <= 256, one slot per group for <= 4096; above
+ * 256 groups a kernel reads 8192 sample rows and picks on the device the slot-table pass (keys
+ * >= 4096 into global atomics), the global path (few passing rows over spread keys) or, above
+ * 4096 groups, a two-pass radix partition of the passing rows into 8-byte records, 2^27 rows at
+ * a time, aggregated per 4096-key partition in a shared slot table; every path gives the same
+ * result), GLOBAL (global atomics for every row). Reads ship, qty, disc, tax, price of dev_cols
+ * and dev_keys; the result accumulates into dev_aggregates[num_groups][6] (caller-zeroed
+ * int128). dev_scratch: device memory of q1_groupkey_scratch_bytes(num_groups), owned by the
+ * caller; calls on different streams need different scratch. A key >= num_groups in a passing
+ * row is reported as Q1_ERR_DOMAIN by q1_sync_check. */
 q1_status q1_launch_groupkey(q1_placement placement, const q1_compressed_columns* dev_cols,
                              const uint32_t* dev_keys, uint32_t num_groups, uint64_t rows,
                              int32_t cutoff_day, const q1_launch_config* cfg, void* dev_scratch,
