@@ -231,15 +231,17 @@ struct CubeTable {
     }
     // Rows r of a quad with bit r of `m` set (passing, key < num_groups, fast domain). All
     // atomics of the quad are issued before any carry is checked, so their latencies overlap.
-    __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
-                                             const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
+    static constexpr bool kPacked = true;
+    // The quantity, discount and tax bytes of the four rows packed in Q, D, X.
+    __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
+                                                    uint32_t X, const uint32_t p[4]) {
         uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4], carry = 0;
         if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            c[r] = key[r] * kCubeDisc + d[r];
-            vx[r] = 1u + (q[r] << 24);   // count + 2^24 * quantity
-            vt[r] = t[r] * p[r];         // < 2^28
+            c[r] = key[r] * kCubeDisc + ((D >> (8 * r)) & 0xFFu);
+            vx[r] = __byte_perm(Q, 1u, 0x0554u | ((uint32_t)r << 12));   // count + 2^24 * quantity
+            vt[r] = ((X >> (8 * r)) & 0xFFu) * p[r];                     // t p < 2^28
             ox[r] = op[r] = ot[r] = 0;
             if ((m >> r) & 1u) {
                 ox[r] = atomicAdd(w + c[r], vx[r]);
@@ -306,14 +308,19 @@ struct Cube3Table {
     __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
         for (uint32_t i = tid; i < kCube3Words * cells; i += nthreads) w[i] = 0;
     }
-    __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
-                                             const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
+    static constexpr bool kPacked = true;
+    // Rows r of a quad with bit r of `m` set (fast domain), the quantity, discount and tax bytes
+    // of the four rows packed in Q, D, X (D and X zero in rows outside the fast domain). There
+    // 9 d + t < 99 fits a byte, so one shift-and-add gives the four (discount, tax) cell offsets.
+    __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
+                                                    uint32_t X, const uint32_t p[4]) {
         uint32_t c[4], vx[4], ox[4], op[4], carry = 0;
         if (!__any_sync(0xffffffffu, m)) return;
+        const uint32_t DT = (D << 3) + D + X;   // bytes r: 9 d + t (garbage outside the fast domain)
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            c[r] = (key[r] * kCubeDisc + d[r]) * kCubeTax + t[r];
-            vx[r] = 1u + (q[r] << 24);   // count + 2^24 * quantity
+            c[r] = key[r] * (kCubeDisc * kCubeTax) + ((DT >> (8 * r)) & 0xFFu);
+            vx[r] = __byte_perm(Q, 1u, 0x0554u | ((uint32_t)r << 12));   // count + 2^24 * quantity
             ox[r] = op[r] = 0;
             if ((m >> r) & 1u) {
                 ox[r] = atomicAdd(w + c[r], vx[r]);
@@ -372,6 +379,7 @@ struct Cube3Table {
 // SlotTable: shared per-group slots for keys < slots
 // ---------------------------------------------------------------------------------------------
 struct SlotTable {
+    static constexpr bool kPacked = false;
     uint32_t* w;       // [kSlotWords][slots]
     uint32_t slots;
     __device__ __forceinline__ void bind(uint8_t* base, uint32_t n) {
@@ -451,17 +459,20 @@ struct SlotTable {
 template <class Table>
 __device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_t num_groups, uint32_t hot,
                                            unsigned long long* acc, uint32_t& bad) {
-    uint32_t q[4], d[4], t[4], m = 0, slow = 0;
+    // rows outside the tables' fast domain: bit 7 of byte r set when d > 10, t > 8 or p >= 2^24
+    const uint32_t top = __byte_perm(__byte_perm(x.p[0], x.p[1], 0x0073u), __byte_perm(x.p[2], x.p[3], 0x0073u),
+                                     0x5410u);   // bytes r: top byte of p[r]
+    const uint32_t outside = (((top & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | top | ((x.D & 0x7F7F7F7Fu) + 0x75757575u) |
+                              x.D | ((x.X & 0x7F7F7F7Fu) + 0x77777777u) | x.X) &
+                             0x80808080u;
+    uint32_t m = 0, slow = 0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        q[r] = (x.Q >> (8 * r)) & 0xFFu;
-        d[r] = (x.D >> (8 * r)) & 0xFFu;
-        t[r] = (x.X >> (8 * r)) & 0xFFu;
         const uint32_t pass = (x.PM >> (8 * r)) & 1u;
         const uint32_t key = x.k[r];
         const uint32_t in = pass & (key < num_groups ? 1u : 0u);
         bad |= pass & (key >= num_groups ? 1u : 0u);
-        const uint32_t fast = in & (key < hot ? 1u : 0u) & (fast_domain(d[r], t[r], x.p[r]) ? 1u : 0u);
+        const uint32_t fast = in & (key < hot ? 1u : 0u) & (((outside >> (8 * r + 7)) & 1u) ^ 1u);
         m |= fast << r;
         slow |= (in & (fast ^ 1u)) << r;
     }
@@ -469,9 +480,25 @@ __device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_
     if (__any_sync(0xffffffffu, slow)) {
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if ((slow >> r) & 1u) scratch_row(acc, x.k[r], q[r], d[r], t[r], x.p[r]);
+            if ((slow >> r) & 1u)
+                scratch_row(acc, x.k[r], (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                            (x.X >> (8 * r)) & 0xFFu, x.p[r]);
     }
-    tab.add_quad(m, x.k, q, d, t, x.p);
+    if constexpr (Table::kPacked) {
+        // discount and tax bytes of in-domain rows only (d <= 10, t <= 8), so that byte-wise
+        // arithmetic on them cannot carry into a neighbouring row's byte
+        const uint32_t inb = ((~outside & 0x80808080u) >> 7) * 0xFFu;
+        tab.add_quad_packed(m, x.k, x.Q, x.D & inb, x.X & inb, x.p);
+    } else {
+        uint32_t q[4], d[4], t[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            q[r] = (x.Q >> (8 * r)) & 0xFFu;
+            d[r] = (x.D >> (8 * r)) & 0xFFu;
+            t[r] = (x.X >> (8 * r)) & 0xFFu;
+        }
+        tab.add_quad(m, x.k, q, d, t, x.p);
+    }
 }
 
 // Barrier of the consumer warps only (the producer keeps streaming): one arrive per warp on an
