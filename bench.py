@@ -33,6 +33,7 @@ sys.path.insert(0, ROOT)
 METRIC = "rows/s & HBM GB/s (% peak), bit-exact; batched/served vs plain, p50/p99 ms"
 UNIT = "rows/s"
 ROWS = 600_000_000
+DEFAULT_ROWS = ROWS
 SEED = 20260102
 BYTES_PER_ROW = 9.25          # 2 + 1 + 1 + 1 + 4 + 2/8
 CUTOFF = 729999
@@ -426,8 +427,11 @@ def main():
               "gpu_launches": launches[0], "clocks": clocks,
               "check": {"groups_count_sum": int(sum(int(merged[g, 0]) for g in range(6)))}}
 
-    if rank == 0 and world == 1 and not args.no_e2e:
-        result["e2e"] = e2e_pinned(q, args)
+    if not args.no_e2e:
+        if world == 1:
+            result["e2e"] = e2e_pinned(q, args)
+        else:   # every rank takes part (a collective); rank 0 reports
+            result["e2e"] = e2e_sharded(q, args, rank, world, local_rank, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
         model, ncpu = cpu_info()
         sample = 50_000_000
@@ -442,6 +446,37 @@ def main():
     if rank == 0:
         print(json.dumps(result), flush=True)
     return 0
+
+
+def e2e_sharded(q, args, rank, world, local_rank, dist):
+    """e2e at N > 1 GPUs (weak scaling): every rank streams its own 600 M-row shard from pinned host
+    memory through q1_run over its own PCIe link (GPU only: filter pushdown and coprocessing would
+    have every rank's host threads contend for the same cores); the job's rows over the slowest
+    rank's time."""
+    import torch
+    ctx = q.Q1Context(device=local_rank, cpu_threads=1)
+    try:
+        from tpchq01_gpu_b200 import shard
+        first_row, rows = shard.shard_rows(ROWS, rank)
+        ctx.generate(SEED, rows, first_row=first_row, layout="compressed", packing="pair", residency="pinned")
+        p = q.Q1Params(hash_table_placement=args.placement, apply_compression=True, num_gpu_streams=4,
+                       num_tuples_per_kernel_launch=1 << 24, num_query_execution_runs=1, cutoff_day=CUTOFF)
+        ctx.run(p)
+        steps = max(3, min(args.steps, 10))
+        dist.barrier()
+        s = time.perf_counter()
+        for _ in range(steps):
+            ctx.run(p)
+        el = torch.tensor([time.perf_counter() - s], device="cuda")
+        dist.all_reduce(el, op=dist.ReduceOp.MAX)
+        t = float(el.item())
+        h2d = int(rows * 9 + 4 * ((rows + 15) // 16)) * world
+        return {"value": world * rows * steps / t, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 576 * world, "steps": steps, "ms_per_step": 1000 * t / steps,
+                "path": f"q1_run on each of {world} ranks, PINNED_HOST residency (its own shard), GPU only, "
+                        "4 streams x 16M-row chunks; the slowest rank's wall time"}
+    finally:
+        ctx.close()
 
 
 def e2e_pinned(q, args):
@@ -515,7 +550,7 @@ def bench_tbl(args):
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
     sh = ctypes.c_void_p(stream.cuda_stream)
-    rows = args.rows if args.rows != ROWS else 6_001_215
+    rows = args.rows if args.rows != DEFAULT_ROWS else 6_001_215
     text = q.tbl_format(q.generate_host(SEED, 0, rows))
     nbytes = len(text)
     dev = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda()
