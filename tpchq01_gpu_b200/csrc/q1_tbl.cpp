@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -20,6 +21,31 @@ using namespace q1;
 
 namespace {
 
+// A stream-ordered memory pool per device that keeps what it frees (the default pool hands freed
+// memory back at every synchronisation, so each call would map its scratch afresh).
+cudaError_t scratch_pool(cudaMemPool_t* pool) {
+    static std::mutex m;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(m);
+    if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if ((e = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return e;
+        uint64_t keep = ~0ull;
+        if ((e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+        pools[dev] = p;
+    }
+    *pool = pools[dev];
+    return cudaSuccess;
+}
+
 struct DeviceMem {
     void* p = nullptr;
     cudaStream_t st = nullptr;   // set: stream-ordered allocation (no device-wide sync on free)
@@ -31,7 +57,8 @@ struct DeviceMem {
     }
     q1_status alloc_async(uint64_t bytes, cudaStream_t stream) {
         if (take_fault(kFaultDeviceAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected device allocation failure");
-        if (cudaMallocAsync(&p, bytes ? bytes : 16, stream) != cudaSuccess) {
+        cudaMemPool_t pool = nullptr;
+        if (scratch_pool(&pool) != cudaSuccess || cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, stream) != cudaSuccess) {
             p = nullptr;
             cudaGetLastError();
             return set_error(Q1_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");

@@ -67,23 +67,36 @@ __device__ __forceinline__ int32_t day_number(int32_t y, int32_t m, int32_t d) {
 
 // Reads a line through a 16-byte window: one aligned 16-byte load per 16 bytes of the line
 // (lanes of a warp read different lines, so every load touches a different cache line; byte
-// loads would cost one L1 wavefront per byte). The last, partial 16-byte block of the buffer is
-// read bytewise so that no load goes past its end.
+// loads would cost one L1 wavefront per byte). Offsets are 32-bit and relative to the line's
+// start (a line whose first eleven fields span more than 2^31 bytes reads as malformed). The
+// last, partial 16-byte block of the buffer is read bytewise so that no load goes past its end.
 struct Cursor {
-    const char* __restrict__ t;
-    uint64_t p, end;
-    uint64_t wbase = ~0ull;   // window: bytes [wbase, wbase + 16) of the address space
+    const char* __restrict__ line;   // the line's first byte
+    const uint4* __restrict__ blk;   // 16-byte blocks from the one holding line[0]
+    uint32_t off;                    // line's offset inside its first block
+    uint32_t p, end;                 // cursor and end of the buffer, relative to line
+    uint32_t full;                   // blocks [0, full) lie wholly inside the buffer
+    uint32_t wi = 0xFFFFFFFFu;       // block in the window
     uint4 win;
+    __device__ __forceinline__ Cursor(const char* __restrict__ text, uint64_t s, uint64_t bytes) {
+        line = text + s;
+        const uintptr_t a = reinterpret_cast<uintptr_t>(line);
+        off = (uint32_t)(a & 15u);
+        blk = reinterpret_cast<const uint4*>(a - off);
+        const uint64_t rest = bytes - s;
+        end = rest < 0x7FFFFFFFull ? (uint32_t)rest : 0x7FFFFFFFu;
+        full = (uint32_t)(((uint64_t)off + end) >> 4);
+        p = 0;
+    }
     __device__ __forceinline__ int peek() {
         if (p >= end) return -1;
-        const uint64_t addr = reinterpret_cast<uint64_t>(t) + p;
-        const uint64_t base = addr & ~15ull;
-        if (base + 16 > reinterpret_cast<uint64_t>(t) + end) return (int)(unsigned char)t[p];
-        if (base != wbase) {
-            win = __ldg(reinterpret_cast<const uint4*>(base));
-            wbase = base;
+        const uint32_t a = off + p, bi = a >> 4;
+        if (bi >= full) return (int)(unsigned char)line[p];
+        if (bi != wi) {
+            win = __ldg(blk + bi);
+            wi = bi;
         }
-        const uint32_t o = (uint32_t)(addr & 15u);
+        const uint32_t o = a & 15u;
         const uint32_t w = o < 8 ? (o < 4 ? win.x : win.y) : (o < 12 ? win.z : win.w);
         return (int)((w >> (8 * (o & 3u))) & 0xFFu);
     }
@@ -161,7 +174,7 @@ struct Out {
 
 // Parses the line starting at byte s into row `row`; false (row zeroed) if malformed.
 __device__ bool parse_line(const char* __restrict__ text, uint64_t bytes, uint64_t s, uint64_t row, const Out& o) {
-    Cursor c{text, s, bytes};
+    Cursor c(text, s, bytes);
     int64_t q = 0, pr = 0, di = 0, tx = 0;
     char rf = 0, ls = 0;
     int32_t ship = 0;
