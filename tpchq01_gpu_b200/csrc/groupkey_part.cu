@@ -179,29 +179,35 @@ __device__ __forceinline__ void partition_quad(Stager& sg, const ka::KeyQuad& x,
                                                uint32_t& bad) {
     using namespace gp;
     const uint32_t G = prm.num_groups;
+    // rows outside the fast domain: bit 7 of byte r set when d > 10, t > 8 or p >= 2^24
+    const uint32_t top = __byte_perm(__byte_perm(x.p[0], x.p[1], 0x0073u), __byte_perm(x.p[2], x.p[3], 0x0073u),
+                                     0x5410u);
+    const uint32_t outside = (((top & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | top | ((x.D & 0x7F7F7F7Fu) + 0x75757575u) |
+                              x.D | ((x.X & 0x7F7F7F7Fu) + 0x77777777u) | x.X) &
+                             0x80808080u;
+    const uint32_t inb = ((~outside & 0x80808080u) >> 7) * 0xFFu;
+    const uint32_t DT = (x.D & inb) | ((x.X & inb) << 4);   // bytes r: d | t << 4 (in-domain rows)
     uint32_t part[4], slow = 0;
     unsigned long long rec[4];
-    uint32_t q[4], d[4], t[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        q[r] = (x.Q >> (8 * r)) & 0xFFu;
-        d[r] = (x.D >> (8 * r)) & 0xFFu;
-        t[r] = (x.X >> (8 * r)) & 0xFFu;
         const uint32_t pass = (x.PM >> (8 * r)) & 1u;
         const uint32_t key = x.k[r];
         const uint32_t in = pass & (key < G ? 1u : 0u);
         bad |= pass & (key >= G ? 1u : 0u);
-        const uint32_t fast = in & (ka::fast_domain(d[r], t[r], x.p[r]) ? 1u : 0u);
+        const uint32_t fast = in & (((outside >> (8 * r + 7)) & 1u) ^ 1u);
         slow |= (in & (fast ^ 1u)) << r;
         part[r] = fast ? key >> kWidthLog : kNoPart;
-        const uint32_t lo = x.p[r] | (q[r] << 24);
-        const uint32_t hi = d[r] | (t[r] << 4) | ((key & (kWidth - 1)) << 8) | 0x80000000u;
+        const uint32_t lo = __byte_perm(x.p[r], x.Q, 0x0210u | ((4u + (uint32_t)r) << 12));   // p | q << 24
+        const uint32_t hi = ((DT >> (8 * r)) & 0xFFu) | ((key & (kWidth - 1)) << 8) | 0x80000000u;
         rec[r] = ((unsigned long long)hi << 32) | lo;
     }
     if (__any_sync(0xffffffffu, slow)) {
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if ((slow >> r) & 1u) ka::scratch_row(prm.acc, x.k[r], q[r], d[r], t[r], x.p[r]);
+            if ((slow >> r) & 1u)
+                ka::scratch_row(prm.acc, x.k[r], (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                                (x.X >> (8 * r)) & 0xFFu, x.p[r]);
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) sg.add(part[r], rec[r], prm);
