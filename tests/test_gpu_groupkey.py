@@ -113,7 +113,8 @@ def test_groupkey_registers(table, num_groups, cutoff):
 
 @pytest.mark.parametrize("num_groups,placement", [
     (4, "in_registers_per_thread"), (7, "in_registers_per_thread"), (6, "shared_mem_per_thread"),
-    (256, "shared_mem_per_thread"), (257, "shared_mem_per_thread"), (3000, "shared_mem_per_thread"),
+    (256, "shared_mem_per_thread"), (257, "shared_mem_per_thread"), (769, "shared_mem_per_thread"),
+    (1024, "shared_mem_per_thread"), (1025, "shared_mem_per_thread"), (3000, "shared_mem_per_thread"),
     (64, "global")])
 def test_domain_edges_take_exact_paths(table, num_groups, placement):
     """Rows with discount > 10, tax > 8, price >= 2^24 or quantity > 50 leave the shared tables'

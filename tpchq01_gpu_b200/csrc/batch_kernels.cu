@@ -11,13 +11,14 @@
 //
 // Per CTA: one producer warp claims items, and for every tile of the item writes the stage's
 // metadata (instance, first row, row count) and streams the six column slices with
-// cp.async.bulk into a 4-stage shared-memory ring (a partial last tile is read by the consumers
+// cp.async.bulk into a shared-memory ring of 4 stages (3 in the table kernel, whose table takes
+// the room of the fourth; a partial last tile is read by the consumers
 // straight from global memory instead). Eight consumer warps aggregate every tile; when the
 // instance changes they flush their accumulators into the instance's scratch (red.global.add),
 // according to the instance's placement mode:
 //   kModeRegisters  num_groups <= 4: per-thread dp4a byte planes (ka::PlaneRegs<4>)
 //   kModeShared     num_groups <= 64: shared (group, discount, tax) cells (ka::Cube3Table);
-//                   <= 256: shared (group, discount) cells (ka::CubeTable); more groups:
+//                   <= 1024: shared (group, discount) cells (ka::CubeTable); more groups:
 //                   shared slots for keys < 2048 (ka::SlotTable), the rest spilled
 //   kModeGlobal     every passing row reduces straight into the scratch accumulators
 // (engines in q1_keyagg.cuh). Scratch per instance: num_groups x 8 u64, folded into the
@@ -38,7 +39,9 @@ using namespace ptx;
 namespace bk {
 
 constexpr uint32_t R = ka::R;   // 2048 rows per tile
-constexpr uint32_t S = 4;
+// ring stages: 4 in the register-planes kernel, 3 in the table kernel
+template <bool kRegs>
+__host__ __device__ constexpr uint32_t stages() { return kRegs ? 4u : 3u; }
 // consumer warps: 8 in the register-planes kernel (128 registers a thread), 16 in the table
 // kernel, whose shared-memory atomics need more warps in flight
 template <bool kRegs>
@@ -46,7 +49,7 @@ __host__ __device__ constexpr uint32_t consumer_warps() { return kRegs ? 8u : 16
 constexpr uint32_t kStage = ka::kStageBytes;
 constexpr uint32_t kSteps = R / 4;
 constexpr uint32_t kKindFull = 0, kKindPartial = 1, kKindEnd = 2;
-// shared table region: the larger of the cube (256 groups) and the slot table (2048 slots)
+// shared table region: the largest of the cubes (64 and 1024 groups) and the slot table (2048 slots)
 constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 constexpr uint32_t kTableBytes =
     cmax(ka::cube3_bytes(ka::kCube3MaxGroups), cmax(ka::cube_bytes(ka::kCubeMaxGroups), ka::slot_bytes(ka::kSlots)));
@@ -77,7 +80,7 @@ struct Current {
 // flushing the engine's accumulators whenever the instance changes and at the end. `k` is the
 // running stage counter shared by all engines of the CTA; returns false if a bounded wait
 // expired (the kernel then stops).
-template <int E, uint32_t W>
+template <int E, uint32_t W, uint32_t S>
 __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t ring, uint8_t* tab, uint64_t* full_bar,
                                                uint64_t* empty_bar, const StageMeta* meta, uint32_t& k,
                                                ka::ConsumerBarrier& cb, uint32_t& bad) {
@@ -200,6 +203,7 @@ __global__ void __launch_bounds__((bk::consumer_warps<kRegs>() + 1) * 32, 1)
     q1_batch_kernel(const __grid_constant__ BatchParams prm) {
     using namespace bk;
     constexpr uint32_t W = consumer_warps<kRegs>();
+    constexpr uint32_t S = stages<kRegs>();
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t full_bar[S];
     __shared__ __align__(8) uint64_t empty_bar[S];
@@ -286,14 +290,14 @@ __global__ void __launch_bounds__((bk::consumer_warps<kRegs>() + 1) * 32, 1)
             const uint32_t e = queue_at<kRegs>(prm, step);
             bool ok;
             if constexpr (kRegs) {
-                ok = consume_engine<kEngRegisters, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad);
+                ok = consume_engine<kEngRegisters, W, S>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad);
             } else {
                 switch (e) {
-                    case kEngCube: ok = consume_engine<kEngCube, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
-                    case kEngSlots: ok = consume_engine<kEngSlots, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
-                    case kEngGlobal: ok = consume_engine<kEngGlobal, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                    case kEngCube: ok = consume_engine<kEngCube, W, S>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                    case kEngSlots: ok = consume_engine<kEngSlots, W, S>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
+                    case kEngGlobal: ok = consume_engine<kEngGlobal, W, S>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad); break;
                     default:   // queues 1 and 0
-                        ok = consume_engine<kEngCube3, W>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad);
+                        ok = consume_engine<kEngCube3, W, S>(prm, ring, tab, full_bar, empty_bar, meta, k, cb, bad);
                         break;
                 }
             }
@@ -356,7 +360,7 @@ cudaError_t launch_batch_zero_outputs(const BatchInstanceDev* inst, const uint64
     return cudaGetLastError();
 }
 
-uint32_t batch_smem_bytes() { return bk::S * bk::kStage + bk::kTableBytes; }
+uint32_t batch_smem_bytes() { return bk::stages<false>() * bk::kStage + bk::kTableBytes; }
 // The register-planes kernel needs only the ring; asking for more than half the SM's shared
 // memory keeps it at one CTA per SM, like the table kernel.
 static uint32_t batch_regs_smem_bytes() { return 120u * 1024u; }

@@ -11,9 +11,10 @@
 // Placements:
 //   in_registers_per_thread  num_groups <= 8: per-thread dp4a byte planes (PlaneRegs<4|8>)
 //   shared_mem_per_thread    num_groups <= 64: shared (group, discount, tax) cells
-//                            (Cube3Table); <= 256: shared (group, discount) cells (CubeTable);
-//                            <= 4096: shared per-group slots (SlotTable, 3-stage ring above
-//                            2048 groups), or, above 4096, this kernel with keys < 4096 in
+//                            (Cube3Table); <= 1024: shared (group, discount) cells (CubeTable,
+//                            3-stage ring above 768 groups); <= 4096: shared per-group slots
+//                            (SlotTable, 3-stage ring above 2048 groups), or, above 4096, this
+//                            kernel with keys < 4096 in
 //                            slots and larger keys reduced straight into the global
 //                            accumulators, or the two-pass partitioned path of
 //                            groupkey_part.cu; above 256 groups the path (and the global
@@ -45,6 +46,7 @@ namespace gk {
 constexpr uint32_t R = ka::R;         // rows per tile
 constexpr uint32_t kMaxStages = 4;    // ring stages (3 when the table needs the room)
 constexpr uint32_t kWideSlots = 4096; // slot-table keys of the single-pass kernel
+constexpr uint32_t kChooseAbove = 256; // the shared placement's path is chosen on the device above
 constexpr uint32_t kMaxDynSmem = 227 * 1024;
 // consumer warps: 8 for the register planes (128 registers a thread), 16 for the shared-table and
 // global placements, whose atomics need more warps in flight to hide their latency
@@ -270,9 +272,9 @@ static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_bl
 }
 
 static uint64_t acc_bytes(uint32_t num_groups) { return 64ull * num_groups; }
-// The shared placement chooses its path on the device above 256 groups (the slot-table sizes).
+// The shared placement chooses its path on the device above 256 groups.
 static bool chosen_on_device(int placement, uint32_t num_groups) {
-    return placement == kPlaceSharedMemPerThread && num_groups > ka::kCubeMaxGroups;
+    return placement == kPlaceSharedMemPerThread && num_groups > gk::kChooseAbove;
 }
 
 // Chooses the path of the shared placement for more than 256 groups from 8192 evenly spaced
@@ -414,7 +416,7 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
 uint64_t groupkey_scratch_bytes(uint32_t num_groups) {
     const uint64_t a = (acc_bytes(num_groups) + 255) & ~255ull;
     if (num_groups >= groupkey_part_min_groups()) return a + groupkey_part_workspace_bytes();
-    if (num_groups > ka::kCubeMaxGroups) return a + 256;   // the path choice's mode word
+    if (num_groups > gk::kChooseAbove) return a + 256;   // the path choice's mode word
     return acc_bytes(num_groups);
 }
 

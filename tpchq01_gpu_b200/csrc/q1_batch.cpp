@@ -98,8 +98,8 @@ void save_cache(const std::string& path) {
 uint32_t q1::batch_engine(uint32_t mode, uint32_t num_groups) {
     if (mode == kModeRegisters && num_groups <= 4) return kEngRegisters;
     if (mode == kModeGlobal) return kEngGlobal;
-    if (num_groups <= 64) return kEngCube3;
-    if (num_groups <= 256) return kEngCube;
+    if (num_groups <= 64) return kEngCube3;     // ka::kCube3MaxGroups
+    if (num_groups <= 1024) return kEngCube;    // ka::kCubeMaxGroups
     return kEngSlots;
 }
 

@@ -9,7 +9,7 @@
 //                  rows per instruction, as in the scan kernel; no atomics until a flush.
 //   Cube3Table     num_groups <= 64: a shared-memory table per (group, discount, tax) cell; a
 //                  row adds its count and quantity (one packed word) and its price: two atomics.
-//   CubeTable      num_groups <= 256: a shared-memory table per (group, discount) cell. A row
+//   CubeTable      num_groups <= 1024: a shared-memory table per (group, discount) cell. A row
 //                  adds only its count and quantity (one packed word), its price and tax * price;
 //                  the discounted sums follow exactly at the flush, because the discount of a
 //                  cell is known there: sum (100-d) p = sum_d (100-d) P_d and
@@ -18,9 +18,16 @@
 //                  kernel, 4096 in the group-key kernel and the partitioned path): count and
 //                  discount packed, quantity, price, disc_price, charge.
 //   global         every row reduces straight into the scratch accumulators.
-// The shared tables use only 32-bit shared atomics (64-bit shared atomics are far slower);
-// 64-bit sums are kept as (low word, carry word) pairs: the low word's atomic returns the old
-// value, and a wrap adds the carry to the high word. Rows outside the tables' fast domain
+// The shared tables use only 32-bit shared atomics (64-bit shared atomics are far slower).
+// The slot table and the (group, discount, tax) cube keep 64-bit sums as (low word, carry word)
+// pairs: the low word's atomic returns the old value, and a wrap adds the carry to the high word.
+// The (group, discount) cube keeps only the low words of its cells, so that 1024 groups fit: a
+// wrap of a cell's packed count-plus-quantity word (about one row in ten) counts in a shared
+// word per group, worth 2^8 units of quantity; a wrap of a price or tax-price word (a few rows in
+// a thousand) adds its 2^32 straight to the group's scratch sums, where the cell's discount fixes
+// what it is worth in each. (The same scheme in the (group, discount, tax) cube measured 3%
+// slower at 64 groups, whose per-group words the frequent quantity wraps contend for.) Rows
+// outside the tables' fast domain
 // (discount > 10, tax > 8 or price >= 2^24; TPC-H data has none) take the global path, so every
 // result is exact over the whole compressed domain.
 //
@@ -58,16 +65,19 @@ __host__ __device__ constexpr uint32_t col_off(int c) {
 constexpr uint32_t kPlaneFlushTiles = 4032;
 constexpr uint64_t kTableFlushRows = 1ull << 23;
 
-constexpr uint32_t kCubeMaxGroups = 256;
+constexpr uint32_t kCubeMaxGroups = 1024;
 constexpr uint32_t kCubeDisc = 11;          // discount 0..10
-constexpr uint32_t kCubeWords = 6;          // xlo xhi plo phi tlo thi
+constexpr uint32_t kCubeWords = 3;          // x p t (low words)
 constexpr uint32_t kCube3MaxGroups = 64;
 constexpr uint32_t kCubeTax = 9;            // tax 0..8
 constexpr uint32_t kCube3Words = 4;         // xlo xhi plo phi
 constexpr uint32_t kSlots = 2048;
 constexpr uint32_t kSlotWords = 9;          // xlo xhi q plo phi dlo dhi clo chi
 
-__host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) { return num_groups * kCubeDisc * kCubeWords * 4; }
+// cells, then (CubeTable) one word per group for the wraps of its count-plus-quantity words
+__host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) {
+    return num_groups * (kCubeDisc * kCubeWords + 1) * 4;
+}
 __host__ __device__ constexpr uint32_t cube3_bytes(uint32_t num_groups) {
     return num_groups * kCubeDisc * kCubeTax * kCube3Words * 4;
 }
@@ -103,6 +113,15 @@ __device__ __forceinline__ void scratch_row(unsigned long long* acc, uint32_t ke
 
 __device__ __forceinline__ bool fast_domain(uint32_t d, uint32_t t, uint32_t p) {
     return d < kCubeDisc && t <= 8u && p < (1u << 24);
+}
+
+// A wrap of a (group, discount) cell's 32-bit price word: 2^32 of price, a 2^32 of disc_price and
+// ab = 100 a 2^32 of charge (a = 100 - d).
+__device__ __forceinline__ void carry_price(unsigned long long* acc, uint32_t g, uint32_t a, uint32_t ab) {
+    unsigned long long* s = acc + 8ull * g;
+    red_add(s + 3, 1ull << 32);
+    red_add(s + 5, a);
+    red_add(s + 7, ab);
 }
 
 // 64-bit sum as (lo, hi) 32-bit shared words: lo += v, carry into hi.
@@ -220,21 +239,24 @@ struct PlaneRegs {
 // CubeTable: shared (group, discount) cells
 // ---------------------------------------------------------------------------------------------
 struct CubeTable {
-    uint32_t* w;       // [kCubeWords][cells]
+    uint32_t* w;       // [kCubeWords][cells]: count + 2^24 quantity, price, tax * price
+    uint32_t* qc;      // [groups]: wraps of the groups' count-plus-quantity words
     uint32_t cells;
     __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
         w = reinterpret_cast<uint32_t*>(base);
         cells = num_groups * kCubeDisc;
+        qc = w + kCubeWords * cells;
     }
     __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
-        for (uint32_t i = tid; i < kCubeWords * cells; i += nthreads) w[i] = 0;
+        for (uint32_t i = tid; i < kCubeWords * cells + cells / kCubeDisc; i += nthreads) w[i] = 0;
     }
     // Rows r of a quad with bit r of `m` set (passing, key < num_groups, fast domain). All
     // atomics of the quad are issued before any carry is checked, so their latencies overlap.
     static constexpr bool kPacked = true;
-    // The quantity, discount and tax bytes of the four rows packed in Q, D, X.
+    // The quantity, discount and tax bytes of the four rows packed in Q, D, X; acc: the scratch
+    // that takes the price words' wraps.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
-                                                    uint32_t X, const uint32_t p[4]) {
+                                                    uint32_t X, const uint32_t p[4], unsigned long long* acc) {
         uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4], carry = 0;
         if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
@@ -245,8 +267,8 @@ struct CubeTable {
             ox[r] = op[r] = ot[r] = 0;
             if ((m >> r) & 1u) {
                 ox[r] = atomicAdd(w + c[r], vx[r]);
-                op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
-                ot[r] = atomicAdd(w + 4 * cells + c[r], vt[r]);
+                op[r] = atomicAdd(w + cells + c[r], p[r]);
+                ot[r] = atomicAdd(w + 2 * cells + c[r], vt[r]);
             }
         }
 #pragma unroll
@@ -259,30 +281,30 @@ struct CubeTable {
         if (__any_sync(0xffffffffu, carry)) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                if ((carry >> (3 * r)) & 1u) atomicAdd(w + cells + c[r], 1u);
-                if ((carry >> (3 * r + 1)) & 1u) atomicAdd(w + 3 * cells + c[r], 1u);
-                if ((carry >> (3 * r + 2)) & 1u) atomicAdd(w + 5 * cells + c[r], 1u);
+                const uint32_t a = 100u - ((D >> (8 * r)) & 0xFFu);
+                if ((carry >> (3 * r)) & 1u) atomicAdd(qc + key[r], 1u);
+                if ((carry >> (3 * r + 1)) & 1u) carry_price(acc, key[r], a, 100u * a);
+                if ((carry >> (3 * r + 2)) & 1u) red_add(acc + 8ull * key[r] + 7, a);
             }
         }
     }
     // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
     __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t tid, uint32_t nthreads) {
         for (uint32_t g = tid; g < num_groups; g += nthreads) {
-            uint64_t cnt = 0, q = 0, dsum = 0, P = 0;
+            uint64_t cnt = 0, q = (uint64_t)qc[g] << 8, dsum = 0, P = 0;
             unsigned __int128 DP = 0, CH = 0;
+            qc[g] = 0;
 #pragma unroll
             for (uint32_t d = 0; d < kCubeDisc; ++d) {
                 const uint32_t c = g * kCubeDisc + d;
-                const uint64_t X = ((uint64_t)w[cells + c] << 32) | w[c];
-                const uint64_t Pd = ((uint64_t)w[3 * cells + c] << 32) | w[2 * cells + c];
-                const uint64_t TPd = ((uint64_t)w[5 * cells + c] << 32) | w[4 * cells + c];
-                const uint64_t nd = X & 0xFFFFFFull;
+                const uint32_t X = w[c], Pd = w[cells + c], TPd = w[2 * cells + c];
+                const uint32_t nd = X & 0xFFFFFFu;
                 cnt += nd;
                 q += X >> 24;
                 dsum += (uint64_t)d * nd;
                 P += Pd;
-                DP += (unsigned __int128)(100u - d) * Pd;
-                CH += (unsigned __int128)(100u - d) * ((unsigned __int128)Pd * 100u + TPd);
+                DP += (uint64_t)(100u - d) * Pd;
+                CH += (unsigned __int128)(100u - d) * ((uint64_t)Pd * 100u + TPd);
 #pragma unroll
                 for (uint32_t k = 0; k < kCubeWords; ++k) w[k * cells + c] = 0;
             }
@@ -313,7 +335,7 @@ struct Cube3Table {
     // of the four rows packed in Q, D, X (D and X zero in rows outside the fast domain). There
     // 9 d + t < 99 fits a byte, so one shift-and-add gives the four (discount, tax) cell offsets.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
-                                                    uint32_t X, const uint32_t p[4]) {
+                                                    uint32_t X, const uint32_t p[4], unsigned long long*) {
         uint32_t c[4], vx[4], ox[4], op[4], carry = 0;
         if (!__any_sync(0xffffffffu, m)) return;
         const uint32_t DT = (D << 3) + D + X;   // bytes r: 9 d + t (garbage outside the fast domain)
@@ -488,7 +510,7 @@ __device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_
         // discount and tax bytes of in-domain rows only (d <= 10, t <= 8), so that byte-wise
         // arithmetic on them cannot carry into a neighbouring row's byte
         const uint32_t inb = ((~outside & 0x80808080u) >> 7) * 0xFFu;
-        tab.add_quad_packed(m, x.k, x.Q, x.D & inb, x.X & inb, x.p);
+        tab.add_quad_packed(m, x.k, x.Q, x.D & inb, x.X & inb, x.p, acc);
     } else {
         uint32_t q[4], d[4], t[4];
 #pragma unroll
