@@ -257,7 +257,7 @@ struct CubeTable {
     // that takes the price words' wraps.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
                                                     uint32_t X, const uint32_t p[4], unsigned long long* acc) {
-        uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4], carry = 0;
+        uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4];
         if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
@@ -271,20 +271,18 @@ struct CubeTable {
                 ot[r] = atomicAdd(w + 2 * cells + c[r], vt[r]);
             }
         }
+        // a word wrapped iff old > ~added (rows not added have old == 0): one predicate, and
+        // the rows only in the rare branch
+        bool wrap = false;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const uint32_t on = (m >> r) & 1u;
-            carry |= (on & (ox[r] + vx[r] < ox[r] ? 1u : 0u)) << (3 * r);
-            carry |= (on & (op[r] + p[r] < op[r] ? 1u : 0u)) << (3 * r + 1);
-            carry |= (on & (ot[r] + vt[r] < ot[r] ? 1u : 0u)) << (3 * r + 2);
-        }
-        if (__any_sync(0xffffffffu, carry)) {
+        for (int r = 0; r < 4; ++r) wrap |= (ox[r] > ~vx[r]) | (op[r] > ~p[r]) | (ot[r] > ~vt[r]);
+        if (__any_sync(0xffffffffu, wrap)) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const uint32_t a = 100u - ((D >> (8 * r)) & 0xFFu);
-                if ((carry >> (3 * r)) & 1u) atomicAdd(qc + key[r], 1u);
-                if ((carry >> (3 * r + 1)) & 1u) carry_price(acc, key[r], a, 100u * a);
-                if ((carry >> (3 * r + 2)) & 1u) red_add(acc + 8ull * key[r] + 7, a);
+                if (ox[r] > ~vx[r]) atomicAdd(qc + key[r], 1u);
+                if (op[r] > ~p[r]) carry_price(acc, key[r], a, 100u * a);
+                if (ot[r] > ~vt[r]) red_add(acc + 8ull * key[r] + 7, a);
             }
         }
     }
@@ -336,7 +334,7 @@ struct Cube3Table {
     // 9 d + t < 99 fits a byte, so one shift-and-add gives the four (discount, tax) cell offsets.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
                                                     uint32_t X, const uint32_t p[4], unsigned long long*) {
-        uint32_t c[4], vx[4], ox[4], op[4], carry = 0;
+        uint32_t c[4], vx[4], ox[4], op[4];
         if (!__any_sync(0xffffffffu, m)) return;
         const uint32_t DT = (D << 3) + D + X;   // bytes r: 9 d + t (garbage outside the fast domain)
 #pragma unroll
@@ -349,18 +347,17 @@ struct Cube3Table {
                 op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
             }
         }
+        // a word wrapped iff old > ~added (rows not added have old == 0): one predicate and
+        // one vote, the rows only in the branch (the count-plus-quantity word wraps about every
+        // tenth row of a cell, the price word every few hundred)
+        bool wrap = false;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const uint32_t on = (m >> r) & 1u;
-            carry |= (on & (ox[r] + vx[r] < ox[r] ? 1u : 0u)) << (2 * r);
-            carry |= (on & (op[r] + p[r] < op[r] ? 1u : 0u)) << (2 * r + 1);
-        }
-        // words wrap rarely (the price word every few hundred rows of a cell): one vote
-        if (__any_sync(0xffffffffu, carry)) {
+        for (int r = 0; r < 4; ++r) wrap |= (ox[r] > ~vx[r]) | (op[r] > ~p[r]);
+        if (__any_sync(0xffffffffu, wrap)) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                if ((carry >> (2 * r)) & 1u) atomicAdd(w + cells + c[r], 1u);
-                if ((carry >> (2 * r + 1)) & 1u) atomicAdd(w + 3 * cells + c[r], 1u);
+                if (ox[r] > ~vx[r]) atomicAdd(w + cells + c[r], 1u);
+                if (op[r] > ~p[r]) atomicAdd(w + 3 * cells + c[r], 1u);
             }
         }
     }
@@ -488,15 +485,24 @@ __device__ __forceinline__ void table_quad(Table& tab, const KeyQuad& x, uint32_
                               x.D | ((x.X & 0x7F7F7F7Fu) + 0x77777777u) | x.X) &
                              0x80808080u;
     uint32_t m = 0, slow = 0;
+    const uint32_t kmax = max(max(x.k[0], x.k[1]), max(x.k[2], x.k[3]));
+    if (kmax < hot) {
+        // every key of the quad in the table (hot <= num_groups): byte-parallel masks, each
+        // gathered to bits 0..3 by one multiply (byte r's bit 0 lands on bit 24 + r)
+        const uint32_t ob = (outside >> 7) * 0xFFu;
+        m = (((x.PM & ~ob) & 0x01010101u) * 0x01020408u) >> 24;
+        slow = (((x.PM & ob) & 0x01010101u) * 0x01020408u) >> 24;
+    } else {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const uint32_t pass = (x.PM >> (8 * r)) & 1u;
-        const uint32_t key = x.k[r];
-        const uint32_t in = pass & (key < num_groups ? 1u : 0u);
-        bad |= pass & (key >= num_groups ? 1u : 0u);
-        const uint32_t fast = in & (key < hot ? 1u : 0u) & (((outside >> (8 * r + 7)) & 1u) ^ 1u);
-        m |= fast << r;
-        slow |= (in & (fast ^ 1u)) << r;
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t pass = (x.PM >> (8 * r)) & 1u;
+            const uint32_t key = x.k[r];
+            const uint32_t in = pass & (key < num_groups ? 1u : 0u);
+            bad |= pass & (key >= num_groups ? 1u : 0u);
+            const uint32_t fast = in & (key < hot ? 1u : 0u) & (((outside >> (8 * r + 7)) & 1u) ^ 1u);
+            m |= fast << r;
+            slow |= (in & (fast ^ 1u)) << r;
+        }
     }
     // rows outside the tables' fast domain (none in TPC-H data): one vote skips the path
     if (__any_sync(0xffffffffu, slow)) {
