@@ -413,7 +413,7 @@ struct SlotTable {
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
         const uint32_t S = slots;
-        uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4], carry = 0;
+        uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4];
         if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
@@ -433,24 +433,24 @@ struct SlotTable {
                 oc[r] = atomicAdd(w + 7 * S + s, cl[r]);
             }
         }
+        // a word wrapped iff old > ~added (rows not added have old == 0): one predicate, and
+        // the rows only in the rare branch
+        bool wrap = false;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const uint32_t on = (m >> r) & 1u;
-            carry |= (on & (ox[r] + vx[r] < ox[r] ? 1u : 0u)) << (3 * r);
-            carry |= (on & (op[r] + p[r] < op[r] ? 1u : 0u)) << (3 * r + 1);
-            carry |= (on & (od[r] + vd[r] < od[r] ? 1u : 0u)) << (3 * r + 2);
-            ch[r] = on ? ch[r] + (oc[r] + cl[r] < oc[r] ? 1u : 0u) : 0u;
+            wrap |= (ox[r] > ~vx[r]) | (op[r] > ~p[r]) | (od[r] > ~vd[r]);
+            ch[r] = ((m >> r) & 1u) ? ch[r] + (oc[r] > ~cl[r] ? 1u : 0u) : 0u;
         }
         // the charge's high word is nonzero for most rows: added per row
 #pragma unroll
         for (int r = 0; r < 4; ++r)
             if (ch[r]) atomicAdd(w + 8 * S + key[r], ch[r]);
-        if (__any_sync(0xffffffffu, carry)) {
+        if (__any_sync(0xffffffffu, wrap)) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                if ((carry >> (3 * r)) & 1u) atomicAdd(w + S + key[r], 1u);
-                if ((carry >> (3 * r + 1)) & 1u) atomicAdd(w + 4 * S + key[r], 1u);
-                if ((carry >> (3 * r + 2)) & 1u) atomicAdd(w + 6 * S + key[r], 1u);
+                if (ox[r] > ~vx[r]) atomicAdd(w + S + key[r], 1u);
+                if (op[r] > ~p[r]) atomicAdd(w + 4 * S + key[r], 1u);
+                if (od[r] > ~vd[r]) atomicAdd(w + 6 * S + key[r], 1u);
             }
         }
     }
