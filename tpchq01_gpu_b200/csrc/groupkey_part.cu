@@ -114,20 +114,20 @@ struct PartParams {
 // The consumer warp's staging state: per partition a 64-record ring in warp-private shared
 // memory, filled at positions handed out by a shared atomic on the partition's tail counter
 // (cheaper than a warp match plus one atomic per partition, even when skewed keys put most
-// lanes in one partition), and drained 32 records (one chunk) at a time from its head. Lane f (< kMaxParts) keeps partition
-// f's head and chunk count in registers.
+// lanes in one partition). The lane whose record takes position 32j + 31 of a partition
+// completes chunk j and has the warp write it out at once, so a ring never holds more than 31
+// unwritten records between calls. Lane f (< kMaxParts) counts partition f's chunks.
 struct Stager {
     unsigned long long* stage;      // [kMaxParts][kStageCap]
     uint32_t* tail;                 // [kMaxParts] records staged so far (shared)
-    uint32_t head;                  // lane f: records of partition f written out
     uint32_t chunks;                // lane f: chunks of partition f written
     uint32_t cur, end;              // current reserved batch [cur, end)
     uint32_t pre;                   // lane 0: first chunk of the prefetched batch
     uint32_t lane;
 
-    // Writes the next up-to-32 staged records of partition f (zero-padded) as one chunk; `tl` is
-    // the partition's tail. All lanes call it with the same f.
-    __device__ __forceinline__ void flush(uint32_t f, uint32_t tl, const PartParams& prm) {
+    // Writes the n <= 32 staged records of partition f from position h on (zero-padded) as one
+    // chunk. All lanes call it with the same f, h, n.
+    __device__ __forceinline__ void flush(uint32_t f, uint32_t h, uint32_t n, const PartParams& prm) {
         using namespace gp;
         if (cur == end) {
             cur = __shfl_sync(0xffffffffu, pre, 0);
@@ -135,8 +135,6 @@ struct Stager {
             if (lane == 0) pre = atomicAdd(&prm.ctl->pool_next, kBatch);
         }
         const uint32_t c = cur++;
-        const uint32_t h = __shfl_sync(0xffffffffu, head, f);
-        const uint32_t n = tl - h;
         const unsigned long long a = stage[f * kStageCap + ((h + lane) & (kStageCap - 1))];
         if (c < prm.pool_cap) {
             prm.pool[(uint64_t)c * kChunk + lane] = lane < n ? a : 0ull;
@@ -145,30 +143,30 @@ struct Stager {
         } else if (lane == 0 && prm.status) {
             atomicOr(prm.status, kStatusInternal);
         }
-        if (lane == f) head = h + (n < kChunk ? n : kChunk);
     }
 
-    // One record per lane (part == kNoPart: none) into the rings; partitions with a full chunk
-    // staged are written out. Before the call every ring holds fewer than 32 records, so the at
-    // most 32 added fit in 64.
+    // One record per lane (part == kNoPart: none) into the rings; chunks completed are written
+    // out. A call adds at most 32 records to a ring that held at most 31, so they fit in 64.
     __device__ __forceinline__ void add(uint32_t part, unsigned long long rec, const PartParams& prm) {
         using namespace gp;
         const bool v = part != kNoPart;
-        if (!__any_sync(0xffffffffu, v)) return;
+        uint32_t pos = 0;
         if (v) {
-            const uint32_t pos = atomicAdd(&tail[part], 1u);
+            pos = atomicAdd(&tail[part], 1u);
             stage[part * kStageCap + (pos & (kStageCap - 1))] = rec;
         }
-        __syncwarp();
-        const uint32_t tl = lane < kMaxParts ? tail[lane] : 0u;
-        uint32_t full = __ballot_sync(0xffffffffu, lane < kMaxParts && tl - head >= kChunk);
+        // positions of one partition in one call are consecutive: at most one completes a chunk
+        uint32_t full = __ballot_sync(0xffffffffu, v && (pos & (kChunk - 1)) == kChunk - 1);
         if (full) {
-            do {
-                const uint32_t f = __ffs(full) - 1;
-                full &= full - 1;
-                flush(f, __shfl_sync(0xffffffffu, tl, f), prm);
-            } while (full);
             __syncwarp();
+            do {
+                const uint32_t l = __ffs(full) - 1;
+                full &= full - 1;
+                const uint32_t f = __shfl_sync(0xffffffffu, part, l);
+                const uint32_t h = __shfl_sync(0xffffffffu, pos, l) - (kChunk - 1);
+                flush(f, h, kChunk, prm);
+            } while (full);
+            __syncwarp();   // the ring slots just read are reused by later calls
         }
     }
 };
@@ -189,15 +187,30 @@ __device__ __forceinline__ void partition_quad(Stager& sg, const ka::KeyQuad& x,
     const uint32_t DT = (x.D & inb) | ((x.X & inb) << 4);   // bytes r: d | t << 4 (in-domain rows)
     uint32_t part[4], slow = 0;
     unsigned long long rec[4];
+    uint32_t fastb;   // byte r = 0xFF: row r becomes a record
+    if (max(max(x.k[0], x.k[1]), max(x.k[2], x.k[3])) < G) {
+        // every key of the quad in range: byte-parallel masks, the slow rows gathered to bits
+        // 0..3 by one multiply (byte r's bit 0 lands on bit 24 + r)
+        const uint32_t ob = (outside >> 7) * 0xFFu;
+        fastb = x.PM & ~ob;
+        slow = (((x.PM & ob) & 0x01010101u) * 0x01020408u) >> 24;
+    } else {
+        fastb = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t pass = (x.PM >> (8 * r)) & 1u;
+            const uint32_t key = x.k[r];
+            const uint32_t in = pass & (key < G ? 1u : 0u);
+            bad |= pass & (key >= G ? 1u : 0u);
+            const uint32_t fast = in & (((outside >> (8 * r + 7)) & 1u) ^ 1u);
+            slow |= (in & (fast ^ 1u)) << r;
+            fastb |= (fast * 0xFFu) << (8 * r);
+        }
+    }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const uint32_t pass = (x.PM >> (8 * r)) & 1u;
         const uint32_t key = x.k[r];
-        const uint32_t in = pass & (key < G ? 1u : 0u);
-        bad |= pass & (key >= G ? 1u : 0u);
-        const uint32_t fast = in & (((outside >> (8 * r + 7)) & 1u) ^ 1u);
-        slow |= (in & (fast ^ 1u)) << r;
-        part[r] = fast ? key >> kWidthLog : kNoPart;
+        part[r] = (fastb >> (8 * r)) & 1u ? key >> kWidthLog : kNoPart;
         const uint32_t lo = __byte_perm(x.p[r], x.Q, 0x0210u | ((4u + (uint32_t)r) << 12));   // p | q << 24
         const uint32_t hi = ((DT >> (8 * r)) & 0xFFu) | ((key & (kWidth - 1)) << 8) | 0x80000000u;
         rec[r] = ((unsigned long long)hi << 32) | lo;
@@ -260,7 +273,6 @@ __global__ void __launch_bounds__((gp::kP1Warps + 1) * 32, 1)
     Stager sg;
     sg.stage = reinterpret_cast<unsigned long long*>(smem + S * kStage) + (uint64_t)warp * kMaxParts * kStageCap;
     sg.tail = tail_s[warp];
-    sg.head = 0;
     sg.chunks = 0;
     sg.cur = sg.end = 0;
     sg.pre = 0;
@@ -292,14 +304,16 @@ __global__ void __launch_bounds__((gp::kP1Warps + 1) * 32, 1)
             partition_quad(sg, i < prm.rows ? ka::load_row(prm.col, i, prm.cutoff, bad) : ka::empty_quad(), prm, bad);
         }
     }
-    // partial chunks, then the reserved chunks left unused
+    // partial chunks (full ones are written as they complete), then the reserved chunks left
+    // unused
     __syncwarp();
     const uint32_t tl = lane < kMaxParts ? sg.tail[lane] : 0u;
-    uint32_t left = __ballot_sync(0xffffffffu, lane < kMaxParts && tl != sg.head);
+    uint32_t left = __ballot_sync(0xffffffffu, lane < kMaxParts && (tl & (kChunk - 1)) != 0u);
     while (left) {
         const uint32_t f = __ffs(left) - 1;
         left &= left - 1;
-        sg.flush(f, __shfl_sync(0xffffffffu, tl, f), prm);
+        const uint32_t t = __shfl_sync(0xffffffffu, tl, f);
+        sg.flush(f, t & ~(kChunk - 1), t & (kChunk - 1), prm);
     }
     const uint32_t p0 = __shfl_sync(0xffffffffu, sg.pre, 0);
     for (uint32_t c = sg.cur + lane; c < sg.end; c += 32)
