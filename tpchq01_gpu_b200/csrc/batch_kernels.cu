@@ -54,7 +54,7 @@ constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 constexpr uint32_t kTableBytes =
     cmax(ka::cube3_bytes(ka::kCube3MaxGroups), cmax(ka::cube_bytes(ka::kCubeMaxGroups), ka::slot_bytes(ka::kSlots)));
 
-struct StageMeta {
+struct __align__(16) StageMeta {
     uint32_t instance;
     uint32_t kind;
     uint32_t rows;     // rows in this tile
@@ -133,14 +133,16 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
         }
     };
 
+    uint32_t s = k % S, ph = (k / S) & 1u;   // stage and phase of stage counter k, stepped below
     for (;; ++k) {
-        const uint32_t s = k % S;
-        const bool landed = mbar_wait(smem_addr(&full_bar[s]), (k / S) & 1u, prm.status);
+        const bool landed = mbar_wait(smem_addr(&full_bar[s]), ph, prm.status);
         if (!__all_sync(0xffffffffu, landed)) {
             ok = false;
             break;
         }
-        const StageMeta m = meta[s];
+        // instance, kind and row count in one 16-byte load (row0 only for a partial tile)
+        const uint4 mh = *reinterpret_cast<const uint4*>(&meta[s]);
+        const StageMeta m{mh.x, mh.y, mh.z, 0u, 0ull};
         if (m.kind == kKindEnd) {
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
@@ -172,11 +174,15 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
             // every lane runs every round (the table engines vote across the warp)
             for (uint32_t i0 = 0; i0 < m.rows; i0 += W * 32) {
                 const uint32_t i = i0 + ctid;
-                add(i < m.rows ? ka::load_row(c.in->col, m.row0 + i, c.cutoff, bad) : ka::empty_quad());
+                add(i < m.rows ? ka::load_row(c.in->col, meta[s].row0 + i, c.cutoff, bad) : ka::empty_quad());
             }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
+        if (++s == S) {
+            s = 0;
+            ph ^= 1u;
+        }
     }
     flush();
     return ok;

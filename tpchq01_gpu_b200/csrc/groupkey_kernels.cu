@@ -138,16 +138,20 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
     if (warp == W) {
         if (lane == 0) {
             const uint64_t pol = policy_evict_first();
-            uint32_t k = 0;
+            // stage s and phase ph of tile k, stepped rather than divided (S is a launch parameter)
+            uint32_t k = 0, s = 0, ph = 0;
             for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {
-                const uint32_t s = k % S;
-                if (!mbar_wait(smem_addr(&empty_bar[s]), ((k / S) & 1u) ^ 1u, prm.status)) break;
+                if (!mbar_wait(smem_addr(&empty_bar[s]), ph ^ 1u, prm.status)) break;
                 const uint32_t fb = smem_addr(&full_bar[s]);
                 mbar_arrive_expect_tx(fb, kStage);
 #pragma unroll
                 for (int c = 0; c < 6; ++c)
                     bulk_g2s(ring + s * kStage + ka::col_off(c), prm.col[c] + t * (uint64_t)ka::col_bytes(c),
                              ka::col_bytes(c), fb, pol);
+                if (++s == S) {
+                    s = 0;
+                    ph ^= 1u;
+                }
             }
             for (uint32_t i = (k > S ? k - S : 0u); i < k; ++i) mbar_wait(smem_addr(&full_bar[i % S]), (i / S) & 1u, prm.status);
         }
@@ -191,10 +195,9 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
         };
 
         bool ok = true;
-        uint32_t k = 0;
-        for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {
-            const uint32_t s = k % S;
-            const bool landed = mbar_wait(smem_addr(&full_bar[s]), (k / S) & 1u, prm.status);
+        uint32_t s = 0, ph = 0;   // stage and phase of the current tile
+        for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+            const bool landed = mbar_wait(smem_addr(&full_bar[s]), ph, prm.status);
             if (!__all_sync(0xffffffffu, landed)) {
                 ok = false;
                 break;
@@ -215,6 +218,10 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
                 add_quad(ka::load_quad(base, ctid + it * (W * 32), prm.cutoff, bad));
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
+            if (++s == S) {
+                s = 0;
+                ph ^= 1u;
+            }
         }
         // the rows after the last full tile, by one CTA straight from global memory
         if (ok && blockIdx.x == (uint32_t)(num_tiles % gridDim.x) && num_tiles * R < prm.rows) {
