@@ -70,6 +70,7 @@ namespace bk {
 // descriptor itself stays in global memory (read through the L1 for flushes and partial tiles).
 struct Current {
     const BatchInstanceDev* in;
+    unsigned long long* acc;   // the instance's scratch accumulators
     uint32_t id;          // instance index, 0xFFFFFFFF before the first
     uint32_t num_groups;
     uint32_t hot;         // keys below `hot` go to the shared table
@@ -90,7 +91,7 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
     ka::CubeTable cube;
     ka::SlotTable slots;
     if constexpr (E == kEngRegisters) regs.zero();
-    Current c{nullptr, 0xFFFFFFFFu, 0, 0, 0};
+    Current c{nullptr, nullptr, 0xFFFFFFFFu, 0, 0, 0};
     uint32_t tiles_since = 0;
     uint64_t rows_since = 0;
     bool ok = true;
@@ -100,12 +101,12 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
         rows_since = 0;
         if (c.id == 0xFFFFFFFFu) return;
         if constexpr (E == kEngRegisters) {
-            regs.flush(c.in->acc, c.num_groups, lane);
+            regs.flush(c.acc, c.num_groups, lane);
         } else if constexpr (E != kEngGlobal) {
             cb.sync(lane, prm.status);
-            if constexpr (E == kEngCube3) cube3.flush(c.in->acc, c.num_groups, ctid, W * 32);
-            else if constexpr (E == kEngCube) cube.flush(c.in->acc, c.num_groups, ctid, W * 32);
-            else slots.flush(c.in->acc, ctid, W * 32);
+            if constexpr (E == kEngCube3) cube3.flush(c.acc, c.num_groups, ctid, W * 32);
+            else if constexpr (E == kEngCube) cube.flush(c.acc, c.num_groups, ctid, W * 32);
+            else slots.flush(c.acc, ctid, W * 32);
             cb.sync(lane, prm.status);
         }
     };
@@ -113,11 +114,11 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
         if constexpr (E == kEngRegisters) {
             regs.add(x, c.num_groups, bad);
         } else if constexpr (E == kEngCube3) {
-            ka::table_quad(cube3, x, c.num_groups, c.hot, c.in->acc, bad);
+            ka::table_quad(cube3, x, c.num_groups, c.hot, c.acc, bad);
         } else if constexpr (E == kEngCube) {
-            ka::table_quad(cube, x, c.num_groups, c.hot, c.in->acc, bad);
+            ka::table_quad(cube, x, c.num_groups, c.hot, c.acc, bad);
         } else if constexpr (E == kEngSlots) {
-            ka::table_quad(slots, x, c.num_groups, c.hot, c.in->acc, bad);
+            ka::table_quad(slots, x, c.num_groups, c.hot, c.acc, bad);
         } else {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
@@ -127,7 +128,7 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
                     bad = 1u;
                     continue;
                 }
-                ka::scratch_row(c.in->acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
+                ka::scratch_row(c.acc, key, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu,
                                 (x.X >> (8 * r)) & 0xFFu, x.p[r]);
             }
         }
@@ -153,6 +154,7 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
             flush();
             c.id = m.instance;
             c.in = prm.inst + m.instance;
+            c.acc = c.in->acc;
             c.num_groups = c.in->num_groups;
             c.cutoff = c.in->cutoff;
             c.hot = (E == kEngSlots && c.num_groups > ka::kSlots) ? ka::kSlots : c.num_groups;

