@@ -349,8 +349,8 @@ uint64_t q1_groupkey_scratch_bytes(uint32_t num_groups);
 
 /* Placements: IN_REGISTERS_PER_THREAD (num_groups <= 8; per-thread byte-plane sums),
  * SHARED_MEM_PER_THREAD (per-CTA shared-memory tables: (group, discount, tax) cells for
- * num_groups <= 64, (group, discount) cells for <= 256, one slot per group for <= 4096; above
- * 256 groups a kernel reads 8192 sample rows and picks on the device the slot-table pass (keys
+ * num_groups <= 64, (group, discount) cells for <= 1024, one slot per group for <= 4096; above
+ * 256 groups a kernel reads 8192 sample rows and picks on the device the shared-table pass (keys
  * >= 4096 into global atomics), the global path (few passing rows over spread keys) or, above
  * 4096 groups, a two-pass radix partition of the passing rows into 8-byte records, 2^27 rows at
  * a time, aggregated per 4096-key partition in a shared slot table; every path gives the same

@@ -45,10 +45,12 @@ def path(request, monkeypatch):
     return request.param
 
 
-@pytest.mark.parametrize("num_groups", [257, 2049, 3000, 4096])
+@pytest.mark.parametrize("num_groups", [257, 1024, 1025, 2049, 3000, 4096])
 @pytest.mark.parametrize("dist", ["uniform", "zipf"])
 @pytest.mark.parametrize("path", ["single", "global", "auto"], indirect=True)
-def test_wide_slots_match_oracle(table, path, num_groups, dist):
+def test_wide_tables_match_oracle(table, path, num_groups, dist):
+    """257..4096 groups: the path is chosen on the device; the single pass keeps (group, discount)
+    cells up to 1024 groups and one slot per group above."""
     comp, c, _ = table
     keys, _ = keys_for(num_groups, dist)
     for cutoff in [727000, 727600, 729999, 730089]:
