@@ -643,6 +643,14 @@ q1_status q1_inject_fault(q1_fault kind, uint32_t count);
  * still usable. */
 q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream);
 
+/* Runs the coprocessing mode's CPU share (the host kernel q1_run gives its CPU fraction) on the
+ * calling thread over rows [begin, end) of compressed columns in HOST memory (the filter field is
+ * not used), adding into aggregates[6][6] (int128, caller-zeroed; same layout as q1_result's
+ * sums, quantity in hundredths). Returns Q1_ERR_DOMAIN when a passing row is outside the kernels'
+ * domain. Needs no GPU; for tests of the host kernel. */
+q1_status q1_selftest_cpu_share(const q1_compressed_columns* host_cols, uint64_t begin, uint64_t end,
+                                int32_t cutoff_day, void* aggregates);
+
 /* One-line description of a CUDA device (name, compute capability, SMs, memory, L2) into buf.
  * Replaces get_device_properties / --device (src/helper.hpp:18-48, src/main.cu:266-268). */
 q1_status q1_device_describe(int32_t device, char* buf, size_t buf_len);

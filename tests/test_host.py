@@ -133,3 +133,62 @@ def test_finalize_averages_truncate_toward_zero():
     assert out[0].avg_qty_e4 == 33333 and out[0].avg_price_e4 == -33333 and out[0].avg_disc_e4 == 233
     assert out[1].avg_qty_e4 == 0 and out[0].returnflag == b"A" and out[3].linestatus == b"O"
     assert out[0].sum_base_price.value() == -1000
+
+
+def _host_cols(c):
+    """q1_compressed_columns over the numpy arrays of a compressed dict (host memory)."""
+    cc = _lib.CompressedColumns()
+    for k in ["shipdate", "discount", "extendedprice", "tax", "quantity"]:
+        setattr(cc, k, c[k].ctypes.data)
+    if "flags" in c:
+        cc.flags = c["flags"].ctypes.data
+        cc.flag_packing = 0
+        cc.num_pair_codes = c["num_pair_codes"]
+        for i in range(4):
+            cc.pair_group[i] = int(c["pair_group"][i])
+    else:
+        cc.returnflag = c["returnflag"].ctypes.data
+        cc.linestatus = c["linestatus"].ctypes.data
+        cc.flag_packing = 1
+    return cc
+
+
+def _edge_rows(c, seed, frac=0.02):
+    """Copy with a fraction of rows at the edges of the domain the CPU share accepts: discount
+    11..100, tax 9..255, prices up to 2^32 - 1, quantity 51..255 (the host kernel's slow steps)."""
+    out = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in c.items()}
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(len(out["shipdate"]), max(1, int(frac * len(out["shipdate"]))), replace=False)
+    out["discount"][idx] = rng.integers(0, 101, len(idx))
+    out["tax"][idx] = rng.integers(0, 256, len(idx))
+    out["extendedprice"][idx] = rng.integers(0, 2**32, len(idx), dtype=np.uint64).astype(np.uint32)
+    out["quantity"][idx] = rng.integers(0, 256, len(idx))
+    return out
+
+
+@pytest.mark.parametrize("packing", ["pair", "separate"])
+@pytest.mark.parametrize("edges", [False, True])
+@pytest.mark.parametrize("cutoff", [727000, 728000, 729999, 731000, 800000])
+def test_cpu_share_equals_oracle(packing, edges, cutoff):
+    """The coprocessing CPU share (q1_run's host kernel, vectorised on hosts that offer it) over
+    three unaligned row ranges adds up to the oracle's table over the whole table."""
+    rows = 300_017
+    c = gen_np.compress(gen_np.generate(41, 0, rows), packing)
+    if edges:
+        c = _edge_rows(c, 5 + cutoff)
+    cc = _host_cols(c)
+    buf = np.zeros(6 * 6 * 2, dtype=np.uint64)
+    for b, e in [(0, 37), (37, 150_001), (150_001, rows)]:
+        _lib.check(q.lib().q1_selftest_cpu_share(ctypes.byref(cc), b, e, cutoff, ctypes.c_void_p(buf.ctypes.data)))
+    want, flag = O.q1_compressed(c, cutoff)
+    assert flag == 0
+    assert np.array_equal(O.i128_to_ints(buf, 6), want)
+
+
+def test_cpu_share_reports_out_of_domain():
+    c = gen_np.compress(gen_np.generate(42, 0, 10_000), "pair")
+    c["discount"][5000] = 101
+    cc = _host_cols(c)
+    buf = np.zeros(6 * 6 * 2, dtype=np.uint64)
+    st = q.lib().q1_selftest_cpu_share(ctypes.byref(cc), 0, 10_000, 729999, ctypes.c_void_p(buf.ctypes.data))
+    assert st == 6   # Q1_ERR_DOMAIN

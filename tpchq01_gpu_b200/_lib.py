@@ -233,6 +233,8 @@ SIGNATURES = {
                                      ctypes.POINTER(ctypes.c_uint64)]),
     "q1_inject_fault": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32]),
     "q1_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_uint32, vp]),
+    "q1_selftest_cpu_share": (ctypes.c_int, [ctypes.POINTER(CompressedColumns), ctypes.c_uint64, ctypes.c_uint64,
+                                             ctypes.c_int32, vp]),
     "q1_version": (ctypes.c_char_p, []),
 }
 

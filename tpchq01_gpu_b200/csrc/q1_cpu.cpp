@@ -230,11 +230,151 @@ __attribute__((target("avx512f,avx512bw,avx512dq"))) bool aggregate_pair_avx512(
     return ok;
 }
 
+// Pair layout, 64 rows per step with AVX-512 VNNI and VBMI: the host form of the GPU kernels'
+// byte-plane dot products. Per step the rows' group masks come from the 2-bit codes by two bit
+// extracts, the prices become three byte planes (byte k of rows 0..63, by byte permutes), and
+// (100 - d)(100 + t) two 7-bit planes from a 128-entry byte table indexed by 9 d + t. Then, per
+// group, vpdpbusd adds four rows' byte products into each 32-bit lane: quantity and discount
+// against the group's 0/1 bytes, and every price plane against the 0/1 bytes, 100 - d and the two
+// charge planes: 14 instructions per group for 64 rows. A step with a passing row outside that
+// fast domain (discount > 10, tax > 8 or a price >= 2^24; TPC-H data has none) goes to the 16-row
+// kernel above, so every result stays exact. Steps are staged 64 at a time and the groups visit
+// them in turn, so that one group's 14 accumulators fit in the registers; a lane adds at most
+// 64 x 4 x 255 x 127 < 2^31 before it is folded into 64 bits. Rows [begin, end) with begin and
+// end multiples of 64.
+constexpr uint32_t kVSteps = 64;
+
+struct VnniTables {
+    alignas(64) uint8_t abl[128], abh[128];   // 9 d + t -> low / high 7 bits of (100 - d)(100 + t)
+    alignas(64) uint8_t plane[3][64];         // permute indices: byte k of the price of row j
+    VnniTables() {
+        for (int i = 0; i < 128; ++i) {
+            const int d = i / 9, x = i % 9;
+            const int ab = d <= 10 ? (100 - d) * (100 + x) : 0;
+            abl[i] = (uint8_t)(ab & 127);
+            abh[i] = (uint8_t)(ab >> 7);
+        }
+        for (int k = 0; k < 3; ++k)
+            for (int j = 0; j < 64; ++j) plane[k][j] = (uint8_t)((4 * j + k) & 127);
+    }
+};
+
+__attribute__((target("avx512f,avx512bw,avx512dq"))) inline uint64_t lane_sum(__m512i v) {
+    const __m512i lo = _mm512_cvtepu32_epi64(_mm512_castsi512_si256(v));
+    const __m512i hi = _mm512_cvtepu32_epi64(_mm512_extracti64x4_epi64(v, 1));
+    return (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(lo, hi));
+}
+
+__attribute__((target("avx512f,avx512bw,avx512dq,avx512vnni,avx512vbmi,bmi2,popcnt"))) bool aggregate_pair_vnni(
+    const HostCompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_rel, Agg128* out) {
+    if (cutoff_rel < 0) return true;   // no row passes
+    static const VnniTables tab;
+    const __m512i cut = _mm512_set1_epi16((short)(uint16_t)std::min<int32_t>(cutoff_rel, 65535));
+    const __m512i ones = _mm512_set1_epi8(1), hundred = _mm512_set1_epi8(100), low4 = _mm512_set1_epi8(15);
+    const __m512i ten = _mm512_set1_epi8(10), eight = _mm512_set1_epi8(8), top = _mm512_set1_epi32((int)0xFF000000u);
+    const __m512i abl0 = _mm512_load_si512(tab.abl), abl1 = _mm512_load_si512(tab.abl + 64);
+    const __m512i abh0 = _mm512_load_si512(tab.abh), abh1 = _mm512_load_si512(tab.abh + 64);
+    __m512i pidx[3];
+    for (int k = 0; k < 3; ++k) pidx[k] = _mm512_load_si512(tab.plane[k]);
+    constexpr uint64_t kEven = 0x5555555555555555ull, kOdd = 0xAAAAAAAAAAAAAAAAull;
+    __m512i st[kVSteps][6];   // per step: price planes 0..2, 100 - d, charge planes low, high
+    uint64_t gm[kVSteps][4];  // per step: rows of each 2-bit code that pass
+    bool ok = true;
+    for (uint64_t s0 = begin; s0 < end; s0 += (uint64_t)kVSteps * 64) {
+        const uint32_t ns = (uint32_t)std::min<uint64_t>(kVSteps, (end - s0) / 64);
+        for (uint32_t j = 0; j < ns; ++j) {
+            const uint64_t i = s0 + 64ull * j;
+            const __m512i sh0 = _mm512_loadu_si512(t.ship + i), sh1 = _mm512_loadu_si512(t.ship + i + 32);
+            const uint64_t pass = (uint64_t)_mm512_cmple_epu16_mask(sh0, cut) |
+                                  ((uint64_t)_mm512_cmple_epu16_mask(sh1, cut) << 32);
+            const __m512i D = _mm512_loadu_si512(t.disc + i), X = _mm512_loadu_si512(t.tax + i);
+            const __m512i p0 = _mm512_loadu_si512(t.price + i), p1 = _mm512_loadu_si512(t.price + i + 16);
+            const __m512i p2 = _mm512_loadu_si512(t.price + i + 32), p3 = _mm512_loadu_si512(t.price + i + 48);
+            const uint64_t outside = _mm512_mask_cmpgt_epu8_mask(pass, D, ten) | _mm512_mask_cmpgt_epu8_mask(pass, X, eight);
+            const __m512i por = _mm512_or_si512(_mm512_or_si512(p0, p1), _mm512_or_si512(p2, p3));
+            if (outside || _mm512_test_epi32_mask(por, top)) {
+                ok &= aggregate_pair_avx512(t, i, i + 64, cutoff_rel, out);
+                gm[j][0] = gm[j][1] = gm[j][2] = gm[j][3] = 0;
+                for (int k = 0; k < 6; ++k) st[j][k] = _mm512_setzero_si512();
+                continue;
+            }
+            uint64_t w0, w1;
+            memcpy(&w0, t.flags + i / 16, 8);
+            memcpy(&w1, t.flags + i / 16 + 2, 8);
+            const uint64_t lo = _pext_u64(w0, kEven) | (_pext_u64(w1, kEven) << 32);
+            const uint64_t hi = _pext_u64(w0, kOdd) | (_pext_u64(w1, kOdd) << 32);
+            gm[j][0] = pass & ~lo & ~hi;
+            gm[j][1] = pass & lo & ~hi;
+            gm[j][2] = pass & ~lo & hi;
+            gm[j][3] = pass & lo & hi;
+            for (int k = 0; k < 3; ++k)
+                st[j][k] = _mm512_mask_blend_epi8(0xFFFFFFFF00000000ull, _mm512_permutex2var_epi8(p0, pidx[k], p1),
+                                                  _mm512_permutex2var_epi8(p2, pidx[k], p3));
+            // 9 d + t on 4-bit fields (no carry between bytes; rows outside the domain do not pass)
+            const __m512i d4 = _mm512_and_si512(D, low4), t4 = _mm512_and_si512(X, low4);
+            const __m512i idx = _mm512_add_epi8(_mm512_add_epi8(_mm512_slli_epi16(d4, 3), d4), t4);
+            st[j][3] = _mm512_sub_epi8(hundred, D);
+            st[j][4] = _mm512_permutex2var_epi8(abl0, idx, abl1);
+            st[j][5] = _mm512_permutex2var_epi8(abh0, idx, abh1);
+        }
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t g = t.pair_group[k];
+            if (g >= 6) continue;
+            __m512i aq = _mm512_setzero_si512(), ad = aq, ap[3] = {aq, aq, aq}, aa[3] = {aq, aq, aq},
+                    al[3] = {aq, aq, aq}, ah[3] = {aq, aq, aq};
+            uint64_t cnt = 0;
+            for (uint32_t j = 0; j < ns; ++j) {
+                const uint64_t m = gm[j][k];
+                cnt += (uint64_t)_mm_popcnt_u64(m);
+                const uint64_t i = s0 + 64ull * j;
+                const __m512i w = _mm512_maskz_mov_epi8(m, ones);
+                const __m512i ak = _mm512_maskz_mov_epi8(m, st[j][3]);
+                const __m512i lk = _mm512_maskz_mov_epi8(m, st[j][4]);
+                const __m512i hk = _mm512_maskz_mov_epi8(m, st[j][5]);
+                aq = _mm512_dpbusd_epi32(aq, _mm512_loadu_si512(t.qty + i), w);
+                ad = _mm512_dpbusd_epi32(ad, _mm512_loadu_si512(t.disc + i), w);
+                for (int b = 0; b < 3; ++b) {
+                    ap[b] = _mm512_dpbusd_epi32(ap[b], st[j][b], w);
+                    aa[b] = _mm512_dpbusd_epi32(aa[b], st[j][b], ak);
+                    al[b] = _mm512_dpbusd_epi32(al[b], st[j][b], lk);
+                    ah[b] = _mm512_dpbusd_epi32(ah[b], st[j][b], hk);
+                }
+            }
+            uint64_t P = 0, DP = 0, CH = 0;
+            for (int b = 0; b < 3; ++b) {
+                P += lane_sum(ap[b]) << (8 * b);
+                DP += lane_sum(aa[b]) << (8 * b);
+                CH += (lane_sum(al[b]) + (lane_sum(ah[b]) << 7)) << (8 * b);
+            }
+            u128* r = out->v[g];
+            r[kAggCount] += cnt;
+            r[kAggQty] += lane_sum(aq) * 100u;
+            r[kAggDisc] += lane_sum(ad);
+            r[kAggBasePrice] += P;
+            r[kAggDiscPrice] += DP;
+            r[kAggCharge] += CH;
+        }
+    }
+    return ok;
+}
+
 }  // namespace
 
 bool cpu_aggregate_compressed(const HostCompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_rel, Agg128* out) {
     static const bool avx512 = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
                                __builtin_cpu_supports("avx512dq");
+    static const bool vnni = avx512 && __builtin_cpu_supports("avx512vnni") && __builtin_cpu_supports("avx512vbmi") &&
+                             __builtin_cpu_supports("bmi2") && __builtin_cpu_supports("popcnt");
+    if (vnni && t.pair && end - begin >= 128) {
+        // head and tail around a 64-aligned body
+        const uint64_t b = std::min<uint64_t>(end, (begin + 63) & ~(uint64_t)63);
+        const uint64_t e = std::max<uint64_t>(b, end & ~(uint64_t)63);
+        bool ok = true;
+        if (begin < b) ok &= cpu_aggregate_compressed(t, begin, b, cutoff_rel, out);
+        if (b < e) ok &= aggregate_pair_vnni(t, b, e, cutoff_rel, out);
+        if (e < end) ok &= cpu_aggregate_compressed(t, e, end, cutoff_rel, out);
+        return ok;
+    }
     if (avx512 && t.pair && end - begin >= 64) {
         // scalar head and tail around a 16-aligned body
         const uint64_t b = std::min<uint64_t>(end, (begin + 15) & ~(uint64_t)15);

@@ -636,6 +636,39 @@ q1_status q1_inject_fault(q1_fault kind, uint32_t count) {
     return Q1_OK;
 }
 
+q1_status q1_selftest_cpu_share(const q1_compressed_columns* cols, uint64_t begin, uint64_t end, int32_t cutoff_day,
+                                void* aggregates) {
+    if (!cols || !aggregates || begin > end) return set_error(Q1_ERR_INVALID_ARGUMENT, "null argument or begin > end");
+    if (begin == end) return Q1_OK;
+    HostCompressed h;
+    h.ship = cols->shipdate;
+    h.disc = cols->discount;
+    h.price = cols->extendedprice;
+    h.tax = cols->tax;
+    h.qty = cols->quantity;
+    h.pair = cols->flag_packing == Q1_FLAGS_PAIR_2BIT;
+    if (h.pair) {
+        if (cols->num_pair_codes < 1 || cols->num_pair_codes > 4)
+            return set_error(Q1_ERR_INVALID_ARGUMENT, "num_pair_codes must be 1..4");
+        h.flags = cols->flags;
+        memcpy(h.pair_group, cols->pair_group, 4);
+        for (uint32_t i = 0; i < 4; ++i) {
+            if (i >= cols->num_pair_codes) h.pair_group[i] = h.pair_group[0];
+            if (h.pair_group[i] >= 6) return set_error(Q1_ERR_INVALID_ARGUMENT, "pair_group entries must be < 6");
+        }
+    } else {
+        h.rf = cols->returnflag;
+        h.ls = cols->linestatus;
+    }
+    if (!h.ship || !h.disc || !h.price || !h.tax || !h.qty || (h.pair ? !h.flags : (!h.rf || !h.ls)))
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "missing column");
+    Agg128 a;
+    memcpy(&a, aggregates, sizeof(a));
+    const bool ok = cpu_aggregate_compressed(h, begin, end, cutoff_day - kShipDateFrame, &a);
+    memcpy(aggregates, &a, sizeof(a));
+    return ok ? Q1_OK : set_error(Q1_ERR_DOMAIN, "a passing row is outside the kernels' domain");
+}
+
 q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream) {
     if (limit_us == 0 || limit_us > 2000000) return set_error(Q1_ERR_INVALID_ARGUMENT, "limit must be 1 us .. 2 s");
     int dev = 0;
