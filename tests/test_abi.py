@@ -37,3 +37,17 @@ def test_library_links_the_cuda_runtime_statically():
     import subprocess
     deps = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
     assert "libcudart.so" not in deps
+
+
+def test_groupkey_scratch_sizes_follow_the_header():
+    """q1_groupkey_scratch_bytes: 64 bytes a group, plus a 256-byte word block for the on-device
+    path choice above 256 groups, plus the partition workspace (about 1.1 GB, independent of the
+    row count) above 4096 groups."""
+    f = q.lib().q1_groupkey_scratch_bytes
+    for g in [1, 4, 64, 256]:
+        assert f(g) == 64 * g
+    for g in [257, 1024, 1025, 4096]:
+        assert f(g) == ((64 * g + 255) // 256) * 256 + 256
+    base = f(4097) - ((64 * 4097 + 255) // 256) * 256
+    assert 0.9e9 < base < 1.3e9
+    assert f(65536) - ((64 * 65536 + 255) // 256) * 256 == base
