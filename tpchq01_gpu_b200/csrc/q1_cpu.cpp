@@ -230,15 +230,16 @@ __attribute__((target("avx512f,avx512bw,avx512dq"))) bool aggregate_pair_avx512(
     return ok;
 }
 
-// Pair layout, 64 rows per step with AVX-512 VNNI and VBMI: the host form of the GPU kernels'
-// byte-plane dot products. Per step the rows' group masks come from the 2-bit codes by two bit
-// extracts, the prices become three byte planes (byte k of rows 0..63, by byte permutes), and
+// 64 rows per step with AVX-512 VNNI and VBMI: the host form of the GPU kernels' byte-plane dot
+// products. Per step the rows' group masks come from the flag bits by bit extracts (pair layout:
+// the 2-bit pair codes; separate layout: the 2-bit return flags and the 1-bit line stati), the
+// prices become three byte planes (byte k of rows 0..63, by byte permutes), and
 // (100 - d)(100 + t) two 7-bit planes from a 128-entry byte table indexed by 9 d + t. Then, per
 // group, vpdpbusd adds four rows' byte products into each 32-bit lane: quantity and discount
 // against the group's 0/1 bytes, and every price plane against the 0/1 bytes, 100 - d and the two
 // charge planes: 14 instructions per group for 64 rows. A step with a passing row outside that
 // fast domain (discount > 10, tax > 8 or a price >= 2^24; TPC-H data has none) goes to the 16-row
-// kernel above, so every result stays exact. Steps are staged 64 at a time and the groups visit
+// kernel above (pair layout) or the row loop (separate layout), so every result stays exact. Steps are staged 64 at a time and the groups visit
 // them in turn, so that one group's 14 accumulators fit in the registers; a lane adds at most
 // 64 x 4 x 255 x 127 < 2^31 before it is folded into 64 bits. Rows [begin, end) with begin and
 // end multiples of 64.
@@ -265,8 +266,13 @@ __attribute__((target("avx512f,avx512bw,avx512dq"))) inline uint64_t lane_sum(__
     return (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(lo, hi));
 }
 
-__attribute__((target("avx512f,avx512bw,avx512dq,avx512vnni,avx512vbmi,bmi2,popcnt"))) bool aggregate_pair_vnni(
+bool aggregate_rows(const HostCompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_rel, Agg128* out);
+
+// kPair: pair codes, 4 masks (code k -> group t.pair_group[k]); else 6 masks, one per group.
+template <bool kPair>
+__attribute__((target("avx512f,avx512bw,avx512dq,avx512vnni,avx512vbmi,bmi2,popcnt"))) bool aggregate_vnni(
     const HostCompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_rel, Agg128* out) {
+    constexpr int NG = kPair ? 4 : 6;
     if (cutoff_rel < 0) return true;   // no row passes
     static const VnniTables tab;
     const __m512i cut = _mm512_set1_epi16((short)(uint16_t)std::min<int32_t>(cutoff_rel, 65535));
@@ -278,7 +284,7 @@ __attribute__((target("avx512f,avx512bw,avx512dq,avx512vnni,avx512vbmi,bmi2,popc
     for (int k = 0; k < 3; ++k) pidx[k] = _mm512_load_si512(tab.plane[k]);
     constexpr uint64_t kEven = 0x5555555555555555ull, kOdd = 0xAAAAAAAAAAAAAAAAull;
     __m512i st[kVSteps][6];   // per step: price planes 0..2, 100 - d, charge planes low, high
-    uint64_t gm[kVSteps][4];  // per step: rows of each 2-bit code that pass
+    uint64_t gm[kVSteps][NG]; // per step: rows of each code (pair) or group (separate) that pass
     bool ok = true;
     for (uint64_t s0 = begin; s0 < end; s0 += (uint64_t)kVSteps * 64) {
         const uint32_t ns = (uint32_t)std::min<uint64_t>(kVSteps, (end - s0) / 64);
@@ -293,20 +299,35 @@ __attribute__((target("avx512f,avx512bw,avx512dq,avx512vnni,avx512vbmi,bmi2,popc
             const uint64_t outside = _mm512_mask_cmpgt_epu8_mask(pass, D, ten) | _mm512_mask_cmpgt_epu8_mask(pass, X, eight);
             const __m512i por = _mm512_or_si512(_mm512_or_si512(p0, p1), _mm512_or_si512(p2, p3));
             if (outside || _mm512_test_epi32_mask(por, top)) {
-                ok &= aggregate_pair_avx512(t, i, i + 64, cutoff_rel, out);
-                gm[j][0] = gm[j][1] = gm[j][2] = gm[j][3] = 0;
+                ok &= kPair ? aggregate_pair_avx512(t, i, i + 64, cutoff_rel, out)
+                            : aggregate_rows(t, i, i + 64, cutoff_rel, out);
+                for (int k = 0; k < NG; ++k) gm[j][k] = 0;
                 for (int k = 0; k < 6; ++k) st[j][k] = _mm512_setzero_si512();
                 continue;
             }
             uint64_t w0, w1;
-            memcpy(&w0, t.flags + i / 16, 8);
-            memcpy(&w1, t.flags + i / 16 + 2, 8);
+            memcpy(&w0, (kPair ? t.flags : t.rf) + i / 16, 8);
+            memcpy(&w1, (kPair ? t.flags : t.rf) + i / 16 + 2, 8);
             const uint64_t lo = _pext_u64(w0, kEven) | (_pext_u64(w1, kEven) << 32);
             const uint64_t hi = _pext_u64(w0, kOdd) | (_pext_u64(w1, kOdd) << 32);
-            gm[j][0] = pass & ~lo & ~hi;
-            gm[j][1] = pass & lo & ~hi;
-            gm[j][2] = pass & ~lo & hi;
-            gm[j][3] = pass & lo & hi;
+            if constexpr (kPair) {
+                gm[j][0] = pass & ~lo & ~hi;
+                gm[j][1] = pass & lo & ~hi;
+                gm[j][2] = pass & ~lo & hi;
+                gm[j][3] = pass & lo & hi;
+            } else {
+                // return flag codes A=0 N=1 R=2 (3 is no group), line status F=0 O=1:
+                // group 2 rf + ls
+                uint64_t ls;
+                memcpy(&ls, t.ls + i / 32, 8);
+                const uint64_t a = pass & ~lo & ~hi, n = pass & lo & ~hi, r = pass & ~lo & hi;
+                gm[j][0] = a & ~ls;
+                gm[j][1] = a & ls;
+                gm[j][2] = n & ~ls;
+                gm[j][3] = n & ls;
+                gm[j][4] = r & ~ls;
+                gm[j][5] = r & ls;
+            }
             for (int k = 0; k < 3; ++k)
                 st[j][k] = _mm512_mask_blend_epi8(0xFFFFFFFF00000000ull, _mm512_permutex2var_epi8(p0, pidx[k], p1),
                                                   _mm512_permutex2var_epi8(p2, pidx[k], p3));
@@ -317,8 +338,8 @@ __attribute__((target("avx512f,avx512bw,avx512dq,avx512vnni,avx512vbmi,bmi2,popc
             st[j][4] = _mm512_permutex2var_epi8(abl0, idx, abl1);
             st[j][5] = _mm512_permutex2var_epi8(abh0, idx, abh1);
         }
-        for (int k = 0; k < 4; ++k) {
-            const uint32_t g = t.pair_group[k];
+        for (int k = 0; k < NG; ++k) {
+            const uint32_t g = kPair ? t.pair_group[k] : (uint32_t)k;
             if (g >= 6) continue;
             __m512i aq = _mm512_setzero_si512(), ad = aq, ap[3] = {aq, aq, aq}, aa[3] = {aq, aq, aq},
                     al[3] = {aq, aq, aq}, ah[3] = {aq, aq, aq};
@@ -365,13 +386,13 @@ bool cpu_aggregate_compressed(const HostCompressed& t, uint64_t begin, uint64_t 
                                __builtin_cpu_supports("avx512dq");
     static const bool vnni = avx512 && __builtin_cpu_supports("avx512vnni") && __builtin_cpu_supports("avx512vbmi") &&
                              __builtin_cpu_supports("bmi2") && __builtin_cpu_supports("popcnt");
-    if (vnni && t.pair && end - begin >= 128) {
+    if (vnni && end - begin >= 128) {
         // head and tail around a 64-aligned body
         const uint64_t b = std::min<uint64_t>(end, (begin + 63) & ~(uint64_t)63);
         const uint64_t e = std::max<uint64_t>(b, end & ~(uint64_t)63);
         bool ok = true;
         if (begin < b) ok &= cpu_aggregate_compressed(t, begin, b, cutoff_rel, out);
-        if (b < e) ok &= aggregate_pair_vnni(t, b, e, cutoff_rel, out);
+        if (b < e) ok &= t.pair ? aggregate_vnni<true>(t, b, e, cutoff_rel, out) : aggregate_vnni<false>(t, b, e, cutoff_rel, out);
         if (e < end) ok &= cpu_aggregate_compressed(t, e, end, cutoff_rel, out);
         return ok;
     }
@@ -385,6 +406,13 @@ bool cpu_aggregate_compressed(const HostCompressed& t, uint64_t begin, uint64_t 
         if (e < end) ok &= cpu_aggregate_compressed(t, e, end, cutoff_rel, out);
         return ok;
     }
+    return aggregate_rows(t, begin, end, cutoff_rel, out);
+}
+
+namespace {
+
+// One row at a time (heads and tails of the vector kernels, the separate layout without them).
+bool aggregate_rows(const HostCompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_rel, Agg128* out) {
     Partial part;
     bool ok = true;
     for (uint64_t b0 = begin; b0 < end; b0 += kBlock) {
@@ -409,6 +437,8 @@ bool cpu_aggregate_compressed(const HostCompressed& t, uint64_t begin, uint64_t 
     }
     return ok;
 }
+
+}  // namespace
 
 bool cpu_aggregate_uncompressed(const HostUncompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_day,
                                 Agg128* out) {
