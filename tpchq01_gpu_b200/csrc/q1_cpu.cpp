@@ -239,10 +239,10 @@ __attribute__((target("avx512f,avx512bw,avx512dq"))) bool aggregate_pair_avx512(
 // against the group's 0/1 bytes, and every price plane against the 0/1 bytes, 100 - d and the two
 // charge planes: 14 instructions per group for 64 rows. A step with a passing row outside that
 // fast domain (discount > 10, tax > 8 or a price >= 2^24; TPC-H data has none) goes to the 16-row
-// kernel above (pair layout) or the row loop (separate layout), so every result stays exact. Steps are staged 64 at a time and the groups visit
-// them in turn, so that one group's 14 accumulators fit in the registers; a lane adds at most
-// 64 x 4 x 255 x 127 < 2^31 before it is folded into 64 bits. Rows [begin, end) with begin and
-// end multiples of 64.
+// kernel above (pair layout) or the row loop (separate layout), so every result stays exact.
+// Steps are staged 64 at a time and the groups visit them in turn, so that one group's 14
+// accumulators fit in the registers; a lane adds at most 64 x 4 x 255 x 127 < 2^31 before it is
+// folded into 64 bits. Rows [begin, end) with begin and end multiples of 64.
 constexpr uint32_t kVSteps = 64;
 
 struct VnniTables {
