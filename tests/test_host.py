@@ -192,3 +192,24 @@ def test_cpu_share_reports_out_of_domain():
     buf = np.zeros(6 * 6 * 2, dtype=np.uint64)
     st = q.lib().q1_selftest_cpu_share(ctypes.byref(cc), 0, 10_000, 729999, ctypes.c_void_p(buf.ctypes.data))
     assert st == 6   # Q1_ERR_DOMAIN
+
+
+def test_cpu_share_rejects_bad_arguments():
+    c = gen_np.compress(gen_np.generate(43, 0, 1_000), "pair")
+    buf = np.zeros(6 * 6 * 2, dtype=np.uint64)
+    out = ctypes.c_void_p(buf.ctypes.data)
+    L = q.lib()
+    cc = _host_cols(c)
+    assert L.q1_selftest_cpu_share(None, 0, 10, 729999, out) == 1
+    assert L.q1_selftest_cpu_share(ctypes.byref(cc), 10, 5, 729999, out) == 1
+    assert L.q1_selftest_cpu_share(ctypes.byref(cc), 5, 5, 729999, out) == 0   # empty range
+    bad = _host_cols(c)
+    bad.num_pair_codes = 0
+    assert L.q1_selftest_cpu_share(ctypes.byref(bad), 0, 1_000, 729999, out) == 1
+    bad = _host_cols(c)
+    bad.pair_group[0] = 6
+    assert L.q1_selftest_cpu_share(ctypes.byref(bad), 0, 1_000, 729999, out) == 1
+    bad = _host_cols(c)
+    bad.flags = None
+    assert L.q1_selftest_cpu_share(ctypes.byref(bad), 0, 1_000, 729999, out) == 1
+    assert not buf.any()
