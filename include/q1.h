@@ -650,6 +650,9 @@ q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream);
  * domain. Needs no GPU; for tests of the host kernel. */
 q1_status q1_selftest_cpu_share(const q1_compressed_columns* host_cols, uint64_t begin, uint64_t end,
                                 int32_t cutoff_day, void* aggregates);
+/* The same for reference-typed (uncompressed) columns in host memory. */
+q1_status q1_selftest_cpu_share_uncompressed(const q1_columns* host_cols, uint64_t begin, uint64_t end,
+                                             int32_t cutoff_day, void* aggregates);
 
 /* One-line description of a CUDA device (name, compute capability, SMs, memory, L2) into buf.
  * Replaces get_device_properties / --device (src/helper.hpp:18-48, src/main.cu:266-268). */

@@ -213,3 +213,31 @@ def test_cpu_share_rejects_bad_arguments():
     bad.flags = None
     assert L.q1_selftest_cpu_share(ctypes.byref(bad), 0, 1_000, 729999, out) == 1
     assert not buf.any()
+
+
+@pytest.mark.parametrize("edges", [False, True])
+@pytest.mark.parametrize("cutoff", [727000, 728000, 729999, 731000])
+def test_cpu_share_uncompressed_equals_oracle(edges, cutoff):
+    """The CPU share on reference-typed columns (vectorised on hosts that offer it) over three
+    unaligned ranges adds up to the oracle's table; with edges, some rows carry values at the edges
+    of the domain (discount 100, tax 255, prices and quantities up to 2^32 - 1)."""
+    rows = 200_003
+    cols = gen_np.generate(44, 0, rows)
+    cols = {k: np.ascontiguousarray(v) for k, v in cols.items()}
+    if edges:
+        rng = np.random.default_rng(cutoff)
+        idx = rng.choice(rows, rows // 50, replace=False)
+        cols["discount"][idx] = rng.integers(0, 101, len(idx))
+        cols["tax"][idx] = rng.integers(0, 256, len(idx))
+        cols["extendedprice"][idx] = rng.integers(0, 2**32, len(idx))
+        cols["quantity"][idx] = rng.integers(0, 2**32, len(idx))
+    cc = _lib.Columns()
+    for k in ["shipdate", "discount", "extendedprice", "tax", "quantity", "returnflag", "linestatus"]:
+        setattr(cc, k, cols[k].ctypes.data)
+    buf = np.zeros(6 * 6 * 2, dtype=np.uint64)
+    for b, e in [(0, 13), (13, 100_001), (100_001, rows)]:
+        _lib.check(q.lib().q1_selftest_cpu_share_uncompressed(ctypes.byref(cc), b, e, cutoff,
+                                                               ctypes.c_void_p(buf.ctypes.data)))
+    want, flag = O.q1_uncompressed(cols, cutoff)
+    assert flag == 0
+    assert np.array_equal(O.i128_to_ints(buf, 6), want)

@@ -235,6 +235,8 @@ SIGNATURES = {
     "q1_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_uint32, vp]),
     "q1_selftest_cpu_share": (ctypes.c_int, [ctypes.POINTER(CompressedColumns), ctypes.c_uint64, ctypes.c_uint64,
                                              ctypes.c_int32, vp]),
+    "q1_selftest_cpu_share_uncompressed": (ctypes.c_int, [ctypes.POINTER(Columns), ctypes.c_uint64, ctypes.c_uint64,
+                                                          ctypes.c_int32, vp]),
     "q1_version": (ctypes.c_char_p, []),
 }
 

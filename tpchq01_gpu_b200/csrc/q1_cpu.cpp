@@ -440,8 +440,89 @@ bool aggregate_rows(const HostCompressed& t, uint64_t begin, uint64_t end, int32
 
 }  // namespace
 
+namespace {
+
+// Reference-typed columns, 8 rows per step with AVX-512: the passing rows' group masks from byte
+// compares on the flag characters, the domain test as four unsigned compares, disc_price and
+// charge by 64-bit multiplies, then per group four masked 64-bit adds, count packed above the
+// quantity (bit 48) and the discount above the price (bit 45). Within a block of kBlock rows a
+// lane adds at most 2^12 in-domain rows: quantity and price sums < 2^44, discount sum < 2^19,
+// count <= 2^12, charge < 2^59.2, so every packed field stays exact (out-of-domain rows clear
+// `ok`, and their sums are not used). Rows [begin, end) with begin and end multiples of 8.
+__attribute__((target("avx512f,avx512bw,avx512dq,avx512vl"))) bool aggregate_unc_avx512(const HostUncompressed& t,
+                                                                                       uint64_t begin, uint64_t end,
+                                                                                       int32_t cutoff_day, Agg128* out) {
+    const __m256i cut = _mm256_set1_epi32(cutoff_day);
+    const __m512i hundred = _mm512_set1_epi64(100), cnt1 = _mm512_set1_epi64(1ll << 48);
+    const __m512i max32 = _mm512_set1_epi64(0xFFFFFFFFll), max8 = _mm512_set1_epi64(255);
+    const __m512i low45 = _mm512_set1_epi64((1ll << 45) - 1);
+    const __m128i cR = _mm_set1_epi8('R'), cN = _mm_set1_epi8('N'), cF = _mm_set1_epi8('F');
+    bool ok = true;
+    for (uint64_t b0 = begin; b0 < end; b0 += kBlock) {
+        const uint64_t b1 = std::min(end, b0 + kBlock);
+        __m512i acc[6][4];
+        for (int g = 0; g < 6; ++g)
+            for (int k = 0; k < 4; ++k) acc[g][k] = _mm512_setzero_si512();
+        __mmask8 bad = 0;
+        for (uint64_t i = b0; i < b1; i += 8) {
+            const __mmask8 pass = _mm256_cmple_epi32_mask(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(t.ship + i)), cut);
+            const __m512i Q = _mm512_loadu_si512(t.qty + i), D = _mm512_loadu_si512(t.disc + i);
+            const __m512i X = _mm512_loadu_si512(t.tax + i), P = _mm512_loadu_si512(t.price + i);
+            bad |= _mm512_mask_cmpgt_epu64_mask(pass, Q, max32) | _mm512_mask_cmpgt_epu64_mask(pass, D, hundred) |
+                   _mm512_mask_cmpgt_epu64_mask(pass, X, max8) | _mm512_mask_cmpgt_epu64_mask(pass, P, max32);
+            const __m512i DP = _mm512_mullo_epi64(_mm512_sub_epi64(hundred, D), P);
+            const __m512i CH = _mm512_mullo_epi64(DP, _mm512_add_epi64(hundred, X));
+            const __m512i QC = _mm512_add_epi64(Q, cnt1);
+            const __m512i PD = _mm512_add_epi64(P, _mm512_slli_epi64(D, 45));
+            uint64_t rfw, lsw;
+            memcpy(&rfw, t.rf + i, 8);
+            memcpy(&lsw, t.ls + i, 8);
+            const __m128i rf = _mm_cvtsi64_si128((long long)rfw), ls = _mm_cvtsi64_si128((long long)lsw);
+            // return flag R -> 2, N -> 1, anything else -> 0; line status F -> 0, anything else -> 1
+            const __mmask8 r = (__mmask8)_mm_cmpeq_epi8_mask(rf, cR), n = (__mmask8)_mm_cmpeq_epi8_mask(rf, cN) & ~r;
+            const __mmask8 a = (__mmask8)~(r | n), f = (__mmask8)_mm_cmpeq_epi8_mask(ls, cF), o = (__mmask8)~f;
+            const __mmask8 gm[6] = {(__mmask8)(pass & a & f), (__mmask8)(pass & a & o), (__mmask8)(pass & n & f),
+                                    (__mmask8)(pass & n & o), (__mmask8)(pass & r & f), (__mmask8)(pass & r & o)};
+            for (int g = 0; g < 6; ++g) {
+                acc[g][0] = _mm512_mask_add_epi64(acc[g][0], gm[g], acc[g][0], QC);
+                acc[g][1] = _mm512_mask_add_epi64(acc[g][1], gm[g], acc[g][1], PD);
+                acc[g][2] = _mm512_mask_add_epi64(acc[g][2], gm[g], acc[g][2], DP);
+                acc[g][3] = _mm512_mask_add_epi64(acc[g][3], gm[g], acc[g][3], CH);
+            }
+        }
+        ok &= bad == 0;
+        for (int g = 0; g < 6; ++g) {
+            const uint64_t qc = (uint64_t)_mm512_reduce_add_epi64(acc[g][0]);
+            const uint64_t pr = (uint64_t)_mm512_reduce_add_epi64(_mm512_and_si512(acc[g][1], low45));
+            const uint64_t d = (uint64_t)_mm512_reduce_add_epi64(_mm512_srli_epi64(acc[g][1], 45));
+            u128* o = out->v[g];
+            o[kAggCount] += qc >> 48;
+            o[kAggQty] += qc & ((1ull << 48) - 1);
+            o[kAggBasePrice] += pr;
+            o[kAggDisc] += d;
+            o[kAggDiscPrice] += (uint64_t)_mm512_reduce_add_epi64(acc[g][2]);
+            o[kAggCharge] += (uint64_t)_mm512_reduce_add_epi64(acc[g][3]);
+        }
+    }
+    return ok;
+}
+
+}  // namespace
+
 bool cpu_aggregate_uncompressed(const HostUncompressed& t, uint64_t begin, uint64_t end, int32_t cutoff_day,
                                 Agg128* out) {
+    static const bool avx512 = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512bw") &&
+                               __builtin_cpu_supports("avx512dq") && __builtin_cpu_supports("avx512vl");
+    if (avx512 && end - begin >= 64) {
+        // row loop for the head and tail around an 8-aligned body
+        const uint64_t b = std::min<uint64_t>(end, (begin + 7) & ~(uint64_t)7);
+        const uint64_t e = std::max<uint64_t>(b, end & ~(uint64_t)7);
+        bool ok = true;
+        if (begin < b) ok &= cpu_aggregate_uncompressed(t, begin, b, cutoff_day, out);
+        if (b < e) ok &= aggregate_unc_avx512(t, b, e, cutoff_day, out);
+        if (e < end) ok &= cpu_aggregate_uncompressed(t, e, end, cutoff_day, out);
+        return ok;
+    }
     Partial part;
     bool ok = true;
     for (uint64_t b0 = begin; b0 < end; b0 += kBlock) {

@@ -669,6 +669,27 @@ q1_status q1_selftest_cpu_share(const q1_compressed_columns* cols, uint64_t begi
     return ok ? Q1_OK : set_error(Q1_ERR_DOMAIN, "a passing row is outside the kernels' domain");
 }
 
+q1_status q1_selftest_cpu_share_uncompressed(const q1_columns* cols, uint64_t begin, uint64_t end, int32_t cutoff_day,
+                                             void* aggregates) {
+    if (!cols || !aggregates || begin > end) return set_error(Q1_ERR_INVALID_ARGUMENT, "null argument or begin > end");
+    if (begin == end) return Q1_OK;
+    HostUncompressed h;
+    h.ship = cols->shipdate;
+    h.disc = cols->discount;
+    h.price = cols->extendedprice;
+    h.tax = cols->tax;
+    h.qty = cols->quantity;
+    h.rf = cols->returnflag;
+    h.ls = cols->linestatus;
+    if (!h.ship || !h.disc || !h.price || !h.tax || !h.qty || !h.rf || !h.ls)
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "missing column");
+    Agg128 a;
+    memcpy(&a, aggregates, sizeof(a));
+    const bool ok = cpu_aggregate_uncompressed(h, begin, end, cutoff_day, &a);
+    memcpy(aggregates, &a, sizeof(a));
+    return ok ? Q1_OK : set_error(Q1_ERR_DOMAIN, "a passing row is outside the kernels' domain");
+}
+
 q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream) {
     if (limit_us == 0 || limit_us > 2000000) return set_error(Q1_ERR_INVALID_ARGUMENT, "limit must be 1 us .. 2 s");
     int dev = 0;
