@@ -958,7 +958,7 @@ def bench_batch(args):
 # ad-hoc tables (rows log-uniform in [1e6, 1e8]), half of each kind, grouping (returnflag,
 # linestatus) or 64 keys, cutoff uniform in [1998-06-01, 1998-12-01]. The same arrival trace
 # runs through the batched server and through the plain one-launch-per-request server; both
-# report p50/p99 and rows/s, and a sample of responses is checked against the judge.
+# report p50/p99 and rows/s, and a sample of responses is checked against the plain arbiter path.
 # ------------------------------------------------------------------------------------------
 
 def serve_trace(rate, duration, pool, seed):
@@ -1067,7 +1067,7 @@ def bench_serve(args):
             st = _lib.ServerStats()
             _lib.check(L.q1_server_stats_get(h, ctypes.byref(st)))
             ok = sum(1 for s_, r in results.values() if s_ == 0)
-            # judge: a sample of responses against the plain one-request path, bit for bit
+            # arbiter check: a sample of responses against the plain one-request path, bit for bit
             sample = sorted(results)[:: max(1, len(results) // 64)]
             same = True
             for i in sample:
@@ -1103,7 +1103,7 @@ def bench_serve(args):
                               "scanned_rows_per_s": st.scanned_rows / wall if wall else None,
                               "cache_hits": st.cache_hits, "cache_misses": st.cache_misses,
                               "evictions": st.evictions, "cached_gb": st.cached_bytes / 1e9,
-                              "open_s": open_s, "judge_sample": len(sample), "judge_identical": bool(same),
+                              "open_s": open_s, "arbiter_sample": len(sample), "arbiter_identical": bool(same),
                               "clocks": clocks}
         finally:
             L.q1_server_close(h)
@@ -1112,7 +1112,7 @@ def bench_serve(args):
     out["speedup_capacity_rows_per_s"] = s_["capacity"]["logical_rows_per_s"] / p_["capacity"]["logical_rows_per_s"]
     out["speedup_at_offered_rate_rows_per_s"] = (s_["logical_rows_per_s"] or 0) / max(p_["logical_rows_per_s"] or 1e-9,
                                                                                      1e-9)
-    out["identical"] = s_["judge_identical"] and p_["judge_identical"]
+    out["identical"] = s_["arbiter_identical"] and p_["arbiter_identical"]
     print(json.dumps(out), flush=True)
     return 0 if out["identical"] else 1
 

@@ -610,7 +610,7 @@ q1_status q1_server_reset_stats(q1_server* server);
 
 /* The plain path for one request: one scan launch over its table (q1_launch_compressed for
  * resident FLAGS requests, q1_launch_groupkey otherwise; ad-hoc FLAGS tables are generated in
- * the compressed pair layout for it), synchronous, on a stream of its own. The judge of every
+ * the compressed pair layout for it), synchronous, on a stream of its own. The arbiter of every
  * served response. */
 q1_status q1_server_plain(q1_server* server, const q1_request* req, q1_response* out);
 

@@ -20,7 +20,7 @@
 // one request per round and one plain scan launch per request: the comparison point.
 //
 // q1_server_plain answers one request from scratch (fresh table, plain scan launch) on its own
-// stream and is the judge every served response must equal bit for bit.
+// stream and is the arbiter every served response must equal bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -256,11 +256,11 @@ struct q1_server {
     Pinned h_resp, h_inst, h_items, h_base, h_lookup;
     uint64_t items_cap = 0;
 
-    // plain launches: plain_scratch for Q1_SERVE_PLAIN rounds (dispatcher thread); the judge
-    // (q1_server_plain) has buffers of its own, serialised by judge_m
+    // plain launches: plain_scratch for Q1_SERVE_PLAIN rounds (dispatcher thread); the arbiter
+    // (q1_server_plain) has buffers of its own, serialised by arbiter_m
     Dev plain_scratch;
-    std::mutex judge_m;
-    Dev judge_table, judge_scratch, judge_out;
+    std::mutex arbiter_m;
+    Dev arbiter_table, arbiter_scratch, arbiter_out;
 
     // queue
     std::mutex m;
@@ -771,12 +771,12 @@ q1_status q1_server_plain(q1_server* s, const q1_request* req, q1_response* out)
     Q1_CUDA(cudaSetDevice(s->device));
     const bool flags = req->grouping == Q1_GROUP_FLAGS;
     const uint32_t G = groups_of(*req);
-    std::lock_guard<std::mutex> jl(s->judge_m);
-    if (!s->judge_out.p && (st = s->judge_out.alloc(kRespWords * 8)) != Q1_OK) return st;
-    if (!s->judge_scratch.p && (st = s->judge_scratch.alloc(q1_groupkey_scratch_bytes(kMaxGroups))) != Q1_OK) return st;
+    std::lock_guard<std::mutex> jl(s->arbiter_m);
+    if (!s->arbiter_out.p && (st = s->arbiter_out.alloc(kRespWords * 8)) != Q1_OK) return st;
+    if (!s->arbiter_scratch.p && (st = s->arbiter_scratch.alloc(q1_groupkey_scratch_bytes(kMaxGroups))) != Q1_OK) return st;
     cudaStream_t sm = s->plain_stream;
     const double t0 = now_ms();
-    Q1_CUDA(cudaMemsetAsync(s->judge_out.p, 0, kRespWords * 8, sm));
+    Q1_CUDA(cudaMemsetAsync(s->arbiter_out.p, 0, kRespWords * 8, sm));
     q1_compressed_columns c{};
     const uint32_t* keys = nullptr;
     uint64_t rows = 0;
@@ -788,10 +788,10 @@ q1_status q1_server_plain(q1_server* s, const q1_request* req, q1_response* out)
         // for the (returnflag, linestatus) grouping, else a keyed table
         rows = req->adhoc_rows;
         const TableLayout L(rows);
-        if (L.total > s->judge_table.n) {
-            if ((st = s->judge_table.alloc(TableLayout(s->opts.max_adhoc_rows).total)) != Q1_OK) return st;
+        if (L.total > s->arbiter_table.n) {
+            if ((st = s->arbiter_table.alloc(TableLayout(s->opts.max_adhoc_rows).total)) != Q1_OK) return st;
         }
-        uint8_t* tb = s->judge_table.as<uint8_t>();
+        uint8_t* tb = s->arbiter_table.as<uint8_t>();
         c.shipdate = reinterpret_cast<const uint16_t*>(tb + L.off[0]);
         c.quantity = tb + L.off[1];
         c.discount = tb + L.off[2];
@@ -814,10 +814,10 @@ q1_status q1_server_plain(q1_server* s, const q1_request* req, q1_response* out)
             keys = reinterpret_cast<const uint32_t*>(tb + L.off[5]);
         }
     }
-    if ((st = plain_launch(*req, c, keys, G, rows, s->judge_scratch.p, s->judge_out.as<q1_i128>(), sm)) != Q1_OK)
+    if ((st = plain_launch(*req, c, keys, G, rows, s->arbiter_scratch.p, s->arbiter_out.as<q1_i128>(), sm)) != Q1_OK)
         return st;
     std::vector<unsigned long long> words((size_t)G * 12);
-    Q1_CUDA(cudaMemcpyAsync(words.data(), s->judge_out.p, (size_t)G * 12 * 8, cudaMemcpyDeviceToHost, sm));
+    Q1_CUDA(cudaMemcpyAsync(words.data(), s->arbiter_out.p, (size_t)G * 12 * 8, cudaMemcpyDeviceToHost, sm));
     if ((st = check_device_status(sm, s->di->status)) != Q1_OK) return st;
     memset(out, 0, sizeof(*out));
     out->status = Q1_OK;
