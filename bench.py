@@ -136,35 +136,34 @@ def cpu_info():
     return model, os.cpu_count()
 
 
-def reference_table(rows, seed):
-    """The reference's lineitem filled from the generator (oracle/_ref; test/bench infrastructure)."""
+REF_CHUNK_ROWS = 1 << 25      # 33.5 M rows per chunk of the reference's table
+
+
+def reference_chunks(rows, seed, threads=None, first_row=0):
+    """The reference's KernelX100 (oracle/_ref, built from the reference sources) over `rows` rows
+    of the generator, the inputs generated by the oracle itself (oracle/gen_rows.h) and held as
+    chunks of the reference's compact copy (12 B/row); no product code is loaded."""
     from oracle import py_oracle as O
-    import tpchq01_gpu_b200 as q
-    cols = q.generate_host(seed, 0, rows)
-    return O.RefTable(cols, CUTOFF)
+    return O.RefChunks(seed, first_row, rows, chunk_rows=REF_CHUNK_ROWS, cutoff_day=CUTOFF, threads=threads)
 
 
-def run_reference_cpu(rows, seconds=None, steps=None, warmup=0, threads=None):
-    """Times KernelX100 of the reference on `threads` host threads over `rows` rows."""
-    threads = threads or os.cpu_count() or 1
-    t = reference_table(rows, SEED)
-    try:
-        for _ in range(warmup):
-            t.x100_parallel(threads)
-        times = []
-        t0 = time.perf_counter()
-        while True:
-            s = time.perf_counter()
-            _, rc = t.x100_parallel(threads)
-            times.append(time.perf_counter() - s)
-            if steps is not None and len(times) >= steps:
-                break
-            if seconds is not None and time.perf_counter() - t0 >= seconds and len(times) >= 3:
-                break
-        used = t.threads()
-    finally:
-        t.close()
-    return rows * len(times) / sum(times), used, times
+def time_reference(chunks, seconds=None, steps=None, warmup=0):
+    """Times full passes of KernelX100 over every chunk: (rows/s, threads, pass times, last table)."""
+    for _ in range(warmup):
+        chunks.run()
+    times, table = [], None
+    t0 = time.perf_counter()
+    while True:
+        s = time.perf_counter()
+        table, rc = chunks.run()
+        times.append(time.perf_counter() - s)
+        if rc != 0:
+            raise RuntimeError(f"reference KernelX100 run failed: {rc}")
+        if steps is not None and len(times) >= steps:
+            break
+        if seconds is not None and time.perf_counter() - t0 >= seconds and len(times) >= 3:
+            break
+    return chunks.rows * len(times) / sum(times), chunks.threads(), times, table
 
 
 def reference_comparators(rows=20_000_000, reps=3):
@@ -175,12 +174,10 @@ def reference_comparators(rows=20_000_000, reps=3):
     its table pointers ((int64_t*)&aggr_avx0_count, :178-184) instead of the tables, so it is not
     run."""
     from oracle import py_oracle as O
-    import tpchq01_gpu_b200 as q
-    cols = q.generate_host(SEED, 0, rows)
     out = {}
     for name, shift, fn in [("hyper_1_thread", 0, "hyper"), ("hyper_compact_1_thread", O.HYPER_COMPACT_SHIFT,
                                                              "hyper_compact")]:
-        t = O.RefTable(cols, CUTOFF - shift)
+        t = O.RefTable.generated(SEED, 0, rows, CUTOFF - shift)
         try:
             best = None
             for _ in range(reps):
@@ -267,21 +264,31 @@ def reference_gpu_arm(args):
 
 
 def reference_arm(args, rank):
+    """The reference's own CPU implementation of the path (KernelX100 on all host threads) on
+    this arm's workload: every step is one pass over all 600 M rows (chunks of 33.5 M rows of the
+    reference's compact copy, resident in host memory)."""
     if rank != 0:
         return 0
     if args.ref_gpu:
         return reference_gpu_arm(args)
     model, ncpu = cpu_info()
-    sample = 50_000_000
-    value, used, times = run_reference_cpu(sample, steps=args.steps, warmup=args.warmup)
-    desc = (f"reference KernelX100<kMagic,true,kNoAvx512> (cpu/kernel_x100.hpp) on {used} host threads, "
-            f"{sample:,} rows of the same generator per step ({model})")
+    t0 = time.perf_counter()
+    chunks = reference_chunks(ROWS, SEED)
+    build_s = time.perf_counter() - t0
+    try:
+        value, used, times, _ = time_reference(chunks, steps=args.steps, warmup=args.warmup)
+        nchunks = chunks.chunks()
+    finally:
+        chunks.close()
+    desc = (f"reference KernelX100<kMagic,true,kNoAvx512> (cpu/kernel_x100.hpp) on {used} host threads, all "
+            f"{ROWS:,} rows per step in {nchunks} chunks of its compact copy ({model})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": config_dict(args.gpus, args.placement),
+            "data": "synthetic", "config": dict(config_dict(args.gpus, args.placement), residency="host"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "reference", "sample": desc},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "setup_s": build_s}
     try:
         line["comparators"] = reference_comparators()
     except Exception as e:   # informative only
@@ -301,6 +308,8 @@ def main():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="scan mode: leave out the batched-vs-plain (C3) object")
+    ap.add_argument("--no-serve", action="store_true", help="scan mode: leave out the served-vs-plain (C4) object")
     ap.add_argument("--mode", default="scan", choices=["scan", "c1sweep", "groupkey", "batch", "serve", "tbl"],
                     help="scan: the 600M-row aggregation (default); batch: 256 instances in one persistent "
                          "launch vs one plain launch each; serve: Poisson request stream, served vs plain")
@@ -315,7 +324,7 @@ def main():
                     help="with --impl reference: the reference's own GPU kernels on this GPU instead of its CPU kernels")
     ap.add_argument("--packing", default="pair", choices=["pair", "separate"],
                     help="scan: flag packing of the table (pair 9.25 B/row, separate 9.375 B/row)")
-    ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of Poisson arrivals per arm")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of Poisson arrivals per arm")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: mean requests per second")
     args = ap.parse_args()
     ROWS = args.rows
@@ -433,18 +442,48 @@ def main():
         else:   # every rank takes part (a collective); rank 0 reports
             result["e2e"] = e2e_sharded(q, args, rank, world, local_rank, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
+        # The reference's KernelX100 over the same 600 M rows: the timed CPU baseline, and its
+        # table is the parity check of the GPU table of the timed steps (tolerance 0).
         model, ncpu = cpu_info()
-        sample = 50_000_000
-        v, used, times = run_reference_cpu(sample, seconds=10.0, warmup=1)
+        chunks = reference_chunks(ROWS, SEED)
+        try:
+            v, used, times, ref_table = time_reference(chunks, seconds=8.0, warmup=1)
+            nchunks = chunks.chunks()
+        finally:
+            chunks.close()
         result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": used, "kind": "reference",
-                                  "sample": f"reference KernelX100<kMagic,true,kNoAvx512> on {used} threads, "
-                                            f"{sample:,} rows of the same generator, {len(times)} passes ({model})"}
+                                  "sample": f"reference KernelX100<kMagic,true,kNoAvx512> on {used} threads, all "
+                                            f"{ROWS:,} rows of the same generator per pass ({nchunks} chunks), "
+                                            f"{len(times)} passes ({model})"}
+        identical = all(int(merged[g][a]) == int(ref_table[g][a]) for g in range(6) for a in range(6))
+        result["parity"] = {"rows": ROWS, "identical": bool(identical), "tolerance": 0,
+                            "against": "reference KernelX100 (cpu/kernel_x100.hpp) on the same generated rows, "
+                                       "every group x {count, sum_qty, sum_base_price, sum_disc, "
+                                       "sum_disc_price, sum_charge} as exact integers",
+                            "table": [[str(int(merged[g][a])) for a in range(6)] for g in range(6)]}
     ctx.close()
+    if world == 1:
+        # the metric's second half: batched and served forms against plain launches on this GPU
+        torch.cuda.empty_cache()
+        if not args.no_batch:
+            b = run_batch(args)
+            result["batch"] = {k: b[k] for k in ["config", "batched", "plain_launches", "plain_synchronised",
+                                                 "speedup_vs_plain", "speedup_vs_plain_synchronised", "identical",
+                                                 "clocks"]}
+            result["gpu_launches_batch"] = b["gpu_launches"]
+        if not args.no_serve:
+            result["serve"] = run_serve(args)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+    if result.get("parity", {}).get("identical") is False:
+        print("parity failure: the GPU table differs from the reference's", file=sys.stderr, flush=True)
+        return 1
+    if result.get("batch", {}).get("identical") is False or result.get("serve", {}).get("identical") is False:
+        print("parity failure: a batched or served result differs from the plain launch", file=sys.stderr, flush=True)
+        return 1
     return 0
 
 
@@ -513,15 +552,72 @@ def e2e_pinned(q, args):
         steps = max(3, min(args.steps, 10))
         t = timed(params(best), steps)
         gpu_rows = int(ROWS * (1 - best))
-        h2d = int(gpu_rows * 3 + gpu_rows * 4 + 4 * ((gpu_rows + 31) // 32) + 4 * ((gpu_rows + 15) // 16))
+        cpu_rows = ROWS - gpu_rows
+        bitmap = 4 * ((gpu_rows + 31) // 32)
+        h2d = int(gpu_rows * 3 + gpu_rows * 4 + bitmap + 4 * ((gpu_rows + 15) // 16))
+        step_s = sum(t) / steps
+        # Host-memory bytes of one step: the CPU share reads its rows (9.25 B/row), the bitmap
+        # producer reads the GPU rows' ship dates (2 B/row) and writes the bitmap, and the copy
+        # engines read everything that crosses PCIe.
+        host_bytes = int(cpu_rows * BYTES_PER_ROW + gpu_rows * 2 + bitmap + h2d)
+        peaks = host_stream_peaks(q)
+        roof = {"pcie_h2d_gbs": peaks["pcie_h2d_gbs"], "host_read_gbs": peaks["host_read_gbs"],
+                "host_read_threads": peaks["threads"], "h2d_bytes_per_step": h2d,
+                "host_bytes_per_step": host_bytes, "h2d_achieved_gbs": h2d / step_s / 1e9,
+                "host_achieved_gbs": host_bytes / step_s / 1e9,
+                "how": "pcie_h2d_gbs: best of 5 cudaMemcpyAsync of 2 GiB from pinned host memory (CUDA events); "
+                       "host_read_gbs: best of 3 reads of a 4 GiB host buffer on all host threads "
+                       "(q1_measure_host_read); both in this run"}
+        roof["frac_pcie"] = roof["h2d_achieved_gbs"] / roof["pcie_h2d_gbs"] if roof["pcie_h2d_gbs"] else None
+        roof["frac_host"] = roof["host_achieved_gbs"] / roof["host_read_gbs"] if roof["host_read_gbs"] else None
+        t_pcie = h2d / (roof["pcie_h2d_gbs"] * 1e9) if roof["pcie_h2d_gbs"] else 0.0
+        t_host = host_bytes / (roof["host_read_gbs"] * 1e9) if roof["host_read_gbs"] else 0.0
+        roof["bound"] = "host_memory" if t_host >= t_pcie else "pcie"
+        roof["frac"] = max(t_pcie, t_host) / step_s
         return {"value": ROWS * steps / sum(t), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 576,
-                "steps": steps, "ms_per_step": 1000 * sum(t) / steps,
+                "steps": steps, "ms_per_step": 1000 * step_s,
                 "path": "q1_run, PINNED_HOST residency, use_filter_pushdown + use_coprocessing, 4 streams x 16M-row "
                         "chunks (H2D + scan per chunk), host predicate bitmap and CPU share on "
                         f"{threads} threads",
-                "cpu_fraction": best, "cpu_fraction_sweep_ms": {str(k): 1000 * v for k, v in sweep.items()}}
+                "cpu_fraction": best, "cpu_fraction_sweep_ms": {str(k): 1000 * v for k, v in sweep.items()},
+                "roofline": roof}
     finally:
         ctx.close()
+
+
+def host_stream_peaks(q):
+    """Measured ceilings of the host-streamed mode on this box: pinned host->device copy rate over
+    PCIe and the host's memory read rate on all its threads."""
+    import ctypes
+    import torch
+    from tpchq01_gpu_b200 import _lib
+    n = 2 << 30
+    src = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    src.fill_(1)
+    dst = torch.empty(n, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    best = None
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        dst.copy_(src, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+    del dst, src
+    torch.cuda.empty_cache()
+    import numpy as np
+    buf = np.ones(4 << 30, dtype=np.uint8)
+    threads = os.cpu_count() or 1
+    g = ctypes.c_double()
+    rates = []
+    for _ in range(3):
+        _lib.check(q.lib().q1_measure_host_read(buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes, threads,
+                                                ctypes.byref(g)))
+        rates.append(g.value)
+    del buf
+    return {"pcie_h2d_gbs": n / (best / 1e3) / 1e9, "host_read_gbs": max(rates), "threads": threads}
 
 
 # ------------------------------------------------------------------------------------------
@@ -843,6 +939,14 @@ def batch_instances(n, seed, group_choices=(4, 64, 1024)):
 
 
 def bench_batch(args):
+    line = run_batch(args)
+    print(json.dumps(line), flush=True)
+    return 0 if line["identical"] else 1
+
+
+def run_batch(args):
+    """C3: the 256 instances in one CUDA-graph launch of the persistent batch kernels against one
+    plain q1_launch_groupkey per instance; returns the JSON object (results compared bit for bit)."""
     import ctypes
     import tempfile
     import torch
@@ -949,8 +1053,9 @@ def bench_batch(args):
                                    "note": "one launch per instance, each result checked before the next launch"},
             "speedup_vs_plain": ms_plain / ms_batch, "speedup_vs_plain_synchronised": ms_plain_sync / ms_batch,
             "identical": bool(same), "clocks": clocks, "gpu_launches": args.steps}
-    print(json.dumps(line), flush=True)
-    return 0 if same else 1
+    del keep, outs_b, outs_p, scratch
+    torch.cuda.empty_cache()
+    return line
 
 
 # ------------------------------------------------------------------------------------------
@@ -1021,6 +1126,14 @@ def run_trace(q, _lib, h, arrivals, reqs, limit_s):
 
 
 def bench_serve(args):
+    out = run_serve(args)
+    print(json.dumps(out), flush=True)
+    return 0 if out["identical"] else 1
+
+
+def run_serve(args):
+    """C4: the Poisson trace through the batched server and through the plain one-launch-per-request
+    server (Q1_SERVE_PLAIN); returns the JSON object."""
     import ctypes
     import torch
     import tpchq01_gpu_b200 as q
@@ -1113,8 +1226,7 @@ def bench_serve(args):
     out["speedup_at_offered_rate_rows_per_s"] = (s_["logical_rows_per_s"] or 0) / max(p_["logical_rows_per_s"] or 1e-9,
                                                                                      1e-9)
     out["identical"] = s_["arbiter_identical"] and p_["arbiter_identical"]
-    print(json.dumps(out), flush=True)
-    return 0 if out["identical"] else 1
+    return out
 
 
 if __name__ == "__main__":

@@ -654,6 +654,14 @@ q1_status q1_selftest_cpu_share(const q1_compressed_columns* host_cols, uint64_t
 q1_status q1_selftest_cpu_share_uncompressed(const q1_columns* host_cols, uint64_t begin, uint64_t end,
                                              int32_t cutoff_day, void* aggregates);
 
+/* Reads `bytes` of host memory at host_buf on `threads` host threads (a contiguous slice each,
+ * 16-byte vector loads reduced into a value that is kept) and returns the rate in *gb_per_s
+ * (bytes / wall time, 1e9 bytes per GB). A measurement helper with no reference counterpart: the
+ * host-streamed mode (PINNED_HOST residency, coprocessing) reads every row from host memory, on
+ * the CPU share's cores or by the GPU's copy engines, so this read rate bounds it next to the
+ * PCIe copy rate. Needs no GPU. */
+q1_status q1_measure_host_read(const void* host_buf, uint64_t bytes, int32_t threads, double* gb_per_s);
+
 /* One-line description of a CUDA device (name, compute capability, SMs, memory, L2) into buf.
  * Replaces get_device_properties / --device (src/helper.hpp:18-48, src/main.cu:266-268). */
 q1_status q1_device_describe(int32_t device, char* buf, size_t buf_len);

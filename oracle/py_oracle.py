@@ -55,6 +55,16 @@ def ref():
         r.q1ref_pool_run.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p]
         r.q1ref_pool_threads.argtypes = [ctypes.c_void_p]
         r.q1ref_pool_free.argtypes = [ctypes.c_void_p]
+        r.q1ref_table_generate.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                           ctypes.c_int32]
+        r.q1ref_chunks_new.restype = ctypes.c_void_p
+        r.q1ref_chunks_new.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                       ctypes.c_int32, ctypes.c_int]
+        r.q1ref_chunks_run.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
+        r.q1ref_chunks_threads.argtypes = [ctypes.c_void_p]
+        r.q1ref_chunks_count.restype = ctypes.c_uint64
+        r.q1ref_chunks_count.argtypes = [ctypes.c_void_p]
+        r.q1ref_chunks_free.argtypes = [ctypes.c_void_p]
         _ref = r
     return _ref
 
@@ -78,6 +88,21 @@ def i128_to_ints(buf, groups):
 
 def _c(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
+
+
+def generate(seed, first_row, rows, threads=None):
+    """Reference-typed columns of the seeded generator (oracle/gen_rows.h), built by the oracle
+    itself: int32 day numbers, int64 hundredths / cents, one-byte flags."""
+    threads = threads or os.cpu_count() or 1
+    c = {"shipdate": np.empty(rows, np.int32), "quantity": np.empty(rows, np.int64),
+         "extendedprice": np.empty(rows, np.int64), "discount": np.empty(rows, np.int64),
+         "tax": np.empty(rows, np.int64), "returnflag": np.empty(rows, "S1"), "linestatus": np.empty(rows, "S1")}
+    L = lib()
+    L.oracle_generate.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int] + [ctypes.c_void_p] * 7
+    L.oracle_generate(seed, first_row, rows, threads, *[ptr(c[k]) for k in ["shipdate", "quantity", "extendedprice",
+                                                                            "discount", "tax", "returnflag",
+                                                                            "linestatus"]])
+    return c
 
 
 def q1_uncompressed(cols, cutoff_day=729999):
@@ -151,12 +176,24 @@ class RefTable:
         r = ref()
         n = len(cols["shipdate"])
         self.n = n
-        self.h = r.q1ref_table_new(max(n, 1))
+        self.h = r.q1ref_table_new(n + 1)
+        self.pool = None
+        if n == 0:
+            return
         keep = [_c(cols["shipdate"], np.int32), _c(cols["discount"], np.int64), _c(cols["extendedprice"], np.int64),
                 _c(cols["tax"], np.int64), _c(cols["quantity"], np.int64),
                 _c(cols["returnflag"].view(np.uint8), np.uint8), _c(cols["linestatus"].view(np.uint8), np.uint8)]
         r.q1ref_table_push(self.h, *[ptr(k) for k in keep], n, cutoff_day)
-        self.pool = None
+
+    @classmethod
+    def generated(cls, seed, first_row, rows, cutoff_day=729999):
+        """A table of generator rows pushed by the reference bridge itself (no numpy copy)."""
+        t = cls.__new__(cls)
+        t.n = rows
+        t.pool = None
+        t.h = ref().q1ref_table_new(rows + 1)
+        ref().q1ref_table_generate(t.h, seed, first_row, rows, cutoff_day)
+        return t
 
     def hyper(self):
         buf = np.zeros(NG * NA * 2, dtype=np.uint64)
@@ -195,6 +232,40 @@ class RefTable:
             self.pool = None
         if self.h:
             ref().q1ref_table_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefChunks:
+    """The reference's KernelX100 over rows [first_row, first_row + rows) of the generator, held
+    as chunks of compact copies (12 B/row; see q1ref_chunks_new) and run on `threads` threads."""
+
+    def __init__(self, seed, first_row, rows, chunk_rows=1 << 25, cutoff_day=729999, threads=None):
+        threads = threads or os.cpu_count() or 1
+        self.rows = rows
+        self.h = ref().q1ref_chunks_new(seed, first_row, rows, chunk_rows, cutoff_day, threads)
+        if not self.h:
+            raise ValueError("RefChunks needs at least one row")
+
+    def run(self, morsel=1 << 16):
+        buf = np.zeros(NG * NA * 2, dtype=np.uint64)
+        rc = ref().q1ref_chunks_run(self.h, morsel, ptr(buf))
+        return i128_to_ints(buf, NG), rc
+
+    def threads(self):
+        return ref().q1ref_chunks_threads(self.h)
+
+    def chunks(self):
+        return int(ref().q1ref_chunks_count(self.h))
+
+    def close(self):
+        if self.h:
+            ref().q1ref_chunks_free(self.h)
             self.h = None
 
     def __del__(self):

@@ -27,8 +27,11 @@
  * All outputs are int128 in the product's conventions: sum_qty in hundredths (the compressed
  * inputs carry whole units, so their sums are multiplied by 100 exactly).
  */
+#include <pthread.h>
 #include <stdint.h>
 #include <string.h>
+
+#include "gen_rows.h"
 
 typedef __int128 i128;
 
@@ -272,4 +275,46 @@ uint64_t oracle_parse_tbl(const char* text, uint64_t bytes, int32_t* ship, int64
         start = end + 1;
     }
     return row;
+}
+
+/* ---------------------------------------------------------------------------------------------
+ * Reference-typed columns of rows [first_row, first_row + rows) of the seeded generator
+ * (gen_rows.h), on `threads` host threads (contiguous row ranges per thread).
+ * ------------------------------------------------------------------------------------------- */
+struct gen_job {
+    uint64_t key, first_row, begin, end;
+    int32_t* ship;
+    int64_t *qty, *price, *disc, *tax;
+    char *rf, *ls;
+};
+
+static void* gen_range(void* arg) {
+    const struct gen_job* j = (const struct gen_job*)arg;
+    for (uint64_t i = j->begin; i < j->end; i++)
+        og_row(j->key, j->first_row + i, j->ship + i, j->qty + i, j->price + i, j->disc + i, j->tax + i, j->rf + i,
+               j->ls + i);
+    return 0;
+}
+
+void oracle_generate(uint64_t seed, uint64_t first_row, uint64_t rows, int threads, int32_t* ship, int64_t* qty,
+                     int64_t* price, int64_t* disc, int64_t* tax, char* rf, char* ls) {
+    enum { MAX_THREADS = 64 };
+    if (threads < 1) threads = 1;
+    if (threads > MAX_THREADS) threads = MAX_THREADS;
+    if ((uint64_t)threads > rows) threads = rows ? (int)rows : 1;
+    struct gen_job jobs[MAX_THREADS];
+    pthread_t tid[MAX_THREADS];
+    int started[MAX_THREADS];
+    const uint64_t per = (rows + (uint64_t)threads - 1) / (uint64_t)threads;
+    for (int t = 0; t < threads; t++) {
+        const uint64_t b = (uint64_t)t * per < rows ? (uint64_t)t * per : rows;
+        const uint64_t e = b + per < rows ? b + per : rows;
+        struct gen_job j = {og_key(seed), first_row, b, e, ship, qty, price, disc, tax, rf, ls};
+        jobs[t] = j;
+        started[t] = t > 0 && pthread_create(&tid[t], 0, gen_range, &jobs[t]) == 0;
+        if (t > 0 && !started[t]) gen_range(&jobs[t]);
+    }
+    gen_range(&jobs[0]);
+    for (int t = 1; t < threads; t++)
+        if (started[t]) pthread_join(tid[t], 0);
 }

@@ -19,12 +19,16 @@
 #include <condition_variable>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <random>
 #include <thread>
 #include <vector>
 
+#include <sys/mman.h>
+
+#include "../gen_rows.h"
 #include "common.hpp"
 #include "kernel_hyper.hpp"
 #include "kernel_hyper_compact.hpp"
@@ -175,6 +179,30 @@ int q1ref_table_push(void* t, const int32_t* shipdate, const int64_t* discount, 
 }
 
 uint64_t q1ref_table_rows(void* t) { return ((RefTable*)t)->li.l_extendedprice.cardinality; }
+
+// Appends rows [first_row, first_row + n) of the seeded generator (oracle/gen_rows.h), pushed one
+// value at a time like q1ref_table_push, with the same cutoff shift. No product code is involved.
+int q1ref_table_generate(void* t, uint64_t seed, uint64_t first_row, uint64_t n, int32_t cutoff_day) {
+    RefTable* r = (RefTable*)t;
+    const int32_t shift = 729999 - cutoff_day;
+    const uint64_t key = og_key(seed);
+    for (uint64_t i = 0; i < n; i++) {
+        int32_t ship;
+        int64_t qty, price, disc, tax;
+        char rf, ls;
+        og_row(key, first_row + i, &ship, &qty, &price, &disc, &tax, &rf, &ls);
+        r->li.l_shipdate.Push(ship + shift);
+        r->li.l_discount.Push(disc);
+        r->li.l_extendedprice.Push(price);
+        r->li.l_tax.Push(tax);
+        r->li.l_quantity.Push(qty);
+        r->li.l_returnflag.Push(rf);
+        r->li.l_linestatus.Push(ls);
+        const unsigned rfc = ((rf == 'R') ? 2u : 0u) + ((rf == 'N') ? 1u : 0u);
+        r->present_mask |= 1u << ((rfc << 1) + (ls == 'F' ? 0u : 1u));
+    }
+    return 0;
+}
 
 // KernelHyPer<true> over the whole table. out: [6][6] int128. Returns 1 on int64 overflow.
 int q1ref_hyper(void* t, i128* out) {
@@ -351,6 +379,214 @@ void q1ref_pool_free(void* pool) {
     for (auto& w : p->workers) w.join();
     for (X100* k : p->kernels) delete k;
     delete p;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// KernelX100 over a table too large for the reference's int64 lineitem in one piece (600 M rows
+// take 23 GB there). The rows are generated in chunks, each into its own lineitem, and
+// ComprData::Get (cpu/common.cpp:155-174) builds that chunk's compact int8/int16/int32 copy: the
+// only column data KernelX100::task reads (its scan() pointers are the l_* members that
+// kernel_compact_init sets, cpu/kernel_x100.hpp:44, :154-173; the lineitem itself supplies only
+// the flags' MinMax for the group-id map, :223-224). The chunk's wide pages are then handed back
+// to the OS (madvise; the mapping stays valid), so the whole table costs 12 B/row. A run clears
+// one KernelX100 per thread once, points every kernel's seven compact-column pointers at chunk c,
+// runs chunk c's morsels on all threads, and so on over the chunks; the per-thread tables are
+// then summed as in q1ref_pool_run. Every kernel keeps chunk 0's lineitem for the group-id map,
+// after its flag MinMax are widened to the whole table's (the union of the chunks'), which is
+// what one lineitem holding every row would carry.
+// ---------------------------------------------------------------------------------------------
+
+// IKernel never frees what new_array allocated (cpu/common.cpp:104-111: `m_clean && false`);
+// these release the arrays the bridge knows by name (all aligned_alloc'ed).
+static void free_base_arrays(BaseKernel* k) {
+    void* arrays[] = {k->aggrs0, k->aggr_dsm0_sum_quantity, k->aggr_dsm0_count, k->aggr_dsm0_sum_base_price,
+                      k->aggr_dsm0_sum_disc_price, k->aggr_dsm0_sum_charge, k->aggr_dsm0_sum_disc,
+                      k->aggr_avx0_count, k->aggr_avx0_sum_quantity, k->aggr_avx0_sum_base_price,
+                      k->aggr_avx0_sum_disc_price_lo, k->aggr_avx0_sum_disc_price_hi, k->aggr_avx0_sum_charge_lo,
+                      k->aggr_avx0_sum_charge_hi, k->aggr_avx0_sum_disc};
+    for (void* a : arrays) free(a);
+}
+
+static void free_compact(ComprData* d) {
+    void* arrays[] = {d->l_shipdate, d->l_returnflag, d->l_linestatus, d->l_discount, d->l_tax, d->l_extendedprice,
+                      d->l_quantity};
+    for (void* a : arrays) free(a);
+    free_base_arrays(d);
+    delete d;
+}
+
+template <typename T>
+static void drop_pages(Column<T>& c) {
+    madvise(c.m_ptr, c.m_alloc_size, MADV_DONTNEED);
+}
+
+static void point_at(X100* k, const ComprData* d) {
+    k->l_shipdate = d->l_shipdate;
+    k->l_returnflag = d->l_returnflag;
+    k->l_linestatus = d->l_linestatus;
+    k->l_discount = d->l_discount;
+    k->l_tax = d->l_tax;
+    k->l_extendedprice = d->l_extendedprice;
+    k->l_quantity = d->l_quantity;
+}
+
+struct RefChunks {
+    std::vector<RefTable*> chunks;
+    std::vector<ComprData*> comp;
+    std::vector<X100*> kernels;
+    std::vector<std::thread> workers;
+    std::mutex m;
+    std::condition_variable cv_start, cv_done;
+    uint64_t generation = 0;
+    int running = 0;
+    bool stop = false;
+    uint64_t end = 0, morsel = 1 << 16;
+    std::atomic<uint64_t> cursor{0};
+    unsigned present_mask = 0;
+
+    void work(int id) {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(m);
+                cv_start.wait(lk, [&] { return stop || generation != seen; });
+                if (stop) return;
+                seen = generation;
+            }
+            X100* k = kernels[id];
+            for (;;) {
+                const uint64_t off = cursor.fetch_add(morsel);
+                if (off >= end) break;
+                k->task(off, (end - off < morsel) ? end - off : morsel);
+            }
+            {
+                std::lock_guard<std::mutex> lk(m);
+                if (--running == 0) cv_done.notify_all();
+            }
+        }
+    }
+};
+
+extern "C" {
+
+// Rows [first_row, first_row + rows) of the seeded generator in chunks of chunk_rows, the
+// predicate's cutoff applied by the ship-date shift of q1ref_table_push, `threads` workers.
+// Returns NULL when rows is 0.
+void* q1ref_chunks_new(uint64_t seed, uint64_t first_row, uint64_t rows, uint64_t chunk_rows, int32_t cutoff_day,
+                       int threads) {
+    if (!rows) return nullptr;
+    if (threads < 1) threads = 1;
+    if (!chunk_rows) chunk_rows = 1ull << 24;
+    RefChunks* h = new RefChunks();
+    const uint64_t nchunks = (rows + chunk_rows - 1) / chunk_rows;
+    h->chunks.assign(nchunks, nullptr);
+    h->comp.assign(nchunks, nullptr);
+    std::atomic<uint64_t> next{0};
+    auto build = [&]() {
+        for (;;) {
+            const uint64_t c = next.fetch_add(1);
+            if (c >= nchunks) return;
+            const uint64_t first = c * chunk_rows;
+            const uint64_t n = (rows - first < chunk_rows) ? rows - first : chunk_rows;
+            RefTable* t = new RefTable(n + 1);
+            q1ref_table_generate(t, seed, first_row + first, n, cutoff_day);
+            {
+                std::lock_guard<std::mutex> lk(g_compact_mutex);
+                if (numa_data) numa_data[0] = nullptr;
+                h->comp[c] = ComprData::Get(t->li, 0);
+                numa_data[0] = nullptr;
+                g_compact_owner = nullptr;
+            }
+            drop_pages(t->li.l_shipdate);
+            drop_pages(t->li.l_discount);
+            drop_pages(t->li.l_extendedprice);
+            drop_pages(t->li.l_tax);
+            drop_pages(t->li.l_quantity);
+            drop_pages(t->li.l_returnflag);
+            drop_pages(t->li.l_linestatus);
+            h->chunks[c] = t;
+        }
+    };
+    // at most 8 chunks in their wide form at once
+    const int builders = (int)std::min<uint64_t>(std::min(threads, 8), nchunks);
+    std::vector<std::thread> bt;
+    for (int i = 0; i < builders; i++) bt.emplace_back(build);
+    for (auto& t : bt) t.join();
+    // chunk 0's lineitem, which the kernels keep, takes the flags' MinMax of the whole table
+    lineitem& li0 = h->chunks[0]->li;
+    for (RefTable* t : h->chunks) {
+        h->present_mask |= t->present_mask;
+        const lineitem& li = t->li;
+        li0.l_returnflag.minmax.min = std::min(li0.l_returnflag.minmax.min, li.l_returnflag.minmax.min);
+        li0.l_returnflag.minmax.max = std::max(li0.l_returnflag.minmax.max, li.l_returnflag.minmax.max);
+        li0.l_linestatus.minmax.min = std::min(li0.l_linestatus.minmax.min, li.l_linestatus.minmax.min);
+        li0.l_linestatus.minmax.max = std::max(li0.l_linestatus.minmax.max, li.l_linestatus.minmax.max);
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_compact_mutex);
+        ComprData* saved = numa_data[0];   // numa_data exists: ComprData::Get created it above
+        numa_data[0] = h->comp[0];   // the kernels' constructors take this copy (kernel_compact_init)
+        for (int i = 0; i < threads; i++) h->kernels.push_back(new X100(li0, 0));
+        numa_data[0] = saved;
+    }
+    for (int i = 0; i < threads; i++) h->workers.emplace_back(&RefChunks::work, h, i);
+    return h;
+}
+
+// KernelX100 over every chunk on all threads. out: [6][6] int128. Returns -1 if the x100 group-id
+// map cannot tell two present groups apart.
+int q1ref_chunks_run(void* hh, uint64_t morsel, i128* out) {
+    RefChunks* h = (RefChunks*)hh;
+    for (X100* k : h->kernels) k->Clear();
+    for (size_t c = 0; c < h->chunks.size(); c++) {
+        for (X100* k : h->kernels) point_at(k, h->comp[c]);
+        std::unique_lock<std::mutex> lk(h->m);
+        h->end = h->chunks[c]->li.l_extendedprice.cardinality;
+        h->morsel = morsel ? morsel : (1 << 16);
+        h->cursor.store(0);
+        h->running = (int)h->workers.size();
+        h->generation++;
+        h->cv_start.notify_all();
+        h->cv_done.wait(lk, [&] { return h->running == 0; });
+    }
+    std::vector<AggrHashTable> sum(MAX_GROUPS);
+    memset(sum.data(), 0, sizeof(AggrHashTable) * MAX_GROUPS);
+    for (X100* k : h->kernels) {
+        for (size_t g = 0; g < MAX_GROUPS; g++) {
+            const AggrHashTable& e = k->aggrs0[g];
+            if (!e.count) continue;
+            sum[g].sum_quantity += e.sum_quantity;
+            sum[g].count += e.count;
+            sum[g].sum_base_price += e.sum_base_price;
+            sum[g].sum_disc += e.sum_disc;
+            sum[g].sum_disc_price += e.sum_disc_price;
+            sum[g].sum_charge += e.sum_charge;
+        }
+    }
+    return table_to_groups_x100(h->chunks[0]->li, sum.data(), h->present_mask, out);
+}
+
+int q1ref_chunks_threads(void* hh) { return (int)((RefChunks*)hh)->workers.size(); }
+
+uint64_t q1ref_chunks_count(void* hh) { return ((RefChunks*)hh)->chunks.size(); }
+
+void q1ref_chunks_free(void* hh) {
+    RefChunks* h = (RefChunks*)hh;
+    {
+        std::lock_guard<std::mutex> lk(h->m);
+        h->stop = true;
+        h->cv_start.notify_all();
+    }
+    for (auto& w : h->workers) w.join();
+    for (X100* k : h->kernels) {
+        free_base_arrays(k);
+        delete k;
+    }
+    for (ComprData* d : h->comp) free_compact(d);
+    for (RefTable* t : h->chunks) delete t;
+    delete h;
 }
 
 }  // extern "C"

@@ -51,3 +51,18 @@ def test_groupkey_scratch_sizes_follow_the_header():
     base = f(4097) - ((64 * 4097 + 255) // 256) * 256
     assert 0.9e9 < base < 1.3e9
     assert f(65536) - ((64 * 65536 + 255) // 256) * 256 == base
+
+
+def test_host_read_probe():
+    """q1_measure_host_read reads a host buffer on several threads and reports a positive rate;
+    bad arguments are rejected."""
+    import ctypes
+    import numpy as np
+    from tpchq01_gpu_b200 import _lib
+    L = q.lib()
+    buf = np.ones(64 << 20, dtype=np.uint8)
+    g = ctypes.c_double()
+    assert L.q1_measure_host_read(buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes, 2, ctypes.byref(g)) == 0
+    assert g.value > 0.1
+    assert L.q1_measure_host_read(buf.ctypes.data_as(ctypes.c_void_p), 100, 2, ctypes.byref(g)) == 1
+    assert L.q1_measure_host_read(None, buf.nbytes, 2, ctypes.byref(g)) == 1

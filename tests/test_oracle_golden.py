@@ -71,3 +71,13 @@ def test_oracle_catches_a_planted_mistake():
     cols["discount"][i] = (cols["discount"][i] + 1) % 11
     got, _ = O.q1_uncompressed(cols, c["cutoff_day"])
     assert [[int(v) for v in row] for row in got] != c["hyper"]
+
+
+@pytest.mark.parametrize("seed,first,rows,threads", [(20260101, 0, 200_003, 4), (9, 1 << 40, 1000, 3), (5, 17, 1, 8)])
+def test_oracle_generator_equals_numpy_restatement(seed, first, rows, threads):
+    """oracle/gen_rows.h (the generator the reference arm and the headline parity use) gives the
+    numpy restatement's columns bit for bit."""
+    a = O.generate(seed, first, rows, threads)
+    b = gen_np.generate(seed, first, rows)
+    for k in b:
+        assert np.array_equal(a[k], b[k]), k

@@ -46,3 +46,40 @@ def test_hyper_compact_equals_restatement(seed, rows, cutoff):
     t.close()
     assert flag == 0
     assert np.array_equal(mine, compact)
+
+
+@pytest.mark.parametrize("seed,first,rows", [(201, 0, 100_001), (202, 12_345_678, 7)])
+def test_bridge_generator_equals_pushed_columns(seed, first, rows):
+    """q1ref_table_generate (the oracle's own generator, pushed by the bridge) builds the same
+    lineitem as pushing the numpy restatement's columns."""
+    a = O.RefTable.generated(seed, first, rows)
+    b = O.RefTable(gen_np.generate(seed, first, rows))
+    ha, fa = a.hyper()
+    hb, fb = b.hyper()
+    a.close()
+    b.close()
+    assert fa == 0 and fb == 0
+    assert np.array_equal(ha, hb)
+
+
+@pytest.mark.parametrize("rows,chunk,threads,cutoff", [(1_000_001, 250_000, 3, 729999),
+                                                       (777_777, 1 << 20, 2, 729906),
+                                                       (300_000, 100_000, 4, 728000)])
+def test_chunked_x100_equals_whole_table(rows, chunk, threads, cutoff):
+    """KernelX100 over chunks of compact copies (a ragged last chunk included) gives the table of
+    one lineitem holding every row, run after run."""
+    seed, first = 301, 5
+    whole = O.RefTable(gen_np.generate(seed, first, rows), cutoff)
+    want, rc = whole.x100_parallel(2, morsel=8192)
+    whole.close()
+    assert rc == 0
+    assert np.array_equal(want, O.q1_uncompressed(gen_np.generate(seed, first, rows), cutoff)[0])
+    ch = O.RefChunks(seed, first, rows, chunk_rows=chunk, cutoff_day=cutoff, threads=threads)
+    try:
+        assert ch.chunks() == (rows + chunk - 1) // chunk and ch.threads() == threads
+        for _ in range(2):
+            got, rc = ch.run(morsel=4096)
+            assert rc == 0
+            assert np.array_equal(got, want)
+    finally:
+        ch.close()

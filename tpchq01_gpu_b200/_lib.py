@@ -201,6 +201,7 @@ SIGNATURES = {
     "q1_generate_compressed_device": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
                                                      ctypes.POINTER(CompressedHostOut), vp]),
     "q1_device_describe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t]),
+    "q1_measure_host_read": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "q1_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchInstance), ctypes.c_uint32, ctypes.POINTER(BatchOpts), vp,
                                        ctypes.POINTER(vp)]),
     "q1_batch_run": (ctypes.c_int, [vp, vp]),

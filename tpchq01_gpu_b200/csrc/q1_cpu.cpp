@@ -11,11 +11,57 @@
 #include <cstring>
 #include <exception>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 #include "q1_common.cuh"
 #include "q1_internal.h"
 
 namespace q1 {
+
+// ---------------------------------------------------------------------------------------------
+// Host memory read rate (q1_measure_host_read)
+// ---------------------------------------------------------------------------------------------
+
+// XOR of every 16-byte word of [p, p + bytes) (bytes a multiple of 16, p 16-byte aligned), four
+// independent accumulators so that loads, not the reduction, set the pace.
+static __m128i xor_words(const __m128i* p, uint64_t words) {
+    __m128i a = _mm_setzero_si128(), b = a, c = a, d = a;
+    uint64_t i = 0;
+    for (; i + 4 <= words; i += 4) {
+        a = _mm_xor_si128(a, _mm_load_si128(p + i));
+        b = _mm_xor_si128(b, _mm_load_si128(p + i + 1));
+        c = _mm_xor_si128(c, _mm_load_si128(p + i + 2));
+        d = _mm_xor_si128(d, _mm_load_si128(p + i + 3));
+    }
+    for (; i < words; ++i) a = _mm_xor_si128(a, _mm_load_si128(p + i));
+    return _mm_xor_si128(_mm_xor_si128(a, b), _mm_xor_si128(c, d));
+}
+
+double host_read_gbs(const void* buf, uint64_t bytes, int threads) {
+    const uint64_t skip = (16 - (reinterpret_cast<uintptr_t>(buf) & 15)) & 15;
+    if (bytes <= skip + 16) return 0.0;
+    const __m128i* base = reinterpret_cast<const __m128i*>(static_cast<const uint8_t*>(buf) + skip);
+    const uint64_t words = (bytes - skip) / 16;
+    if (threads < 1) threads = 1;
+    std::vector<std::thread> ts;
+    std::vector<uint64_t> out((size_t)threads);
+    const uint64_t per = (words + (uint64_t)threads - 1) / (uint64_t)threads;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int t = 0; t < threads; ++t) {
+        const uint64_t b = std::min<uint64_t>(words, (uint64_t)t * per), e = std::min<uint64_t>(words, b + per);
+        ts.emplace_back([&out, base, b, e, t] {
+            const __m128i x = xor_words(base + b, e - b);
+            out[(size_t)t] = (uint64_t)_mm_cvtsi128_si64(x) ^ (uint64_t)_mm_cvtsi128_si64(_mm_unpackhi_epi64(x, x));
+        });
+    }
+    for (auto& t : ts) t.join();
+    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    volatile uint64_t sink = 0;
+    for (const uint64_t v : out) sink = sink ^ v;
+    (void)sink;
+    return s > 0 ? (double)(words * 16) / s / 1e9 : 0.0;
+}
 
 // ---------------------------------------------------------------------------------------------
 // Pool

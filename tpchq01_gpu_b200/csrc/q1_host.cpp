@@ -123,6 +123,14 @@ const char* q1_status_string(q1_status s) {
 
 const char* q1_version(void) { return "q1-b200 1.0 (sm_100a)"; }
 
+q1_status q1_measure_host_read(const void* host_buf, uint64_t bytes, int32_t threads, double* gb_per_s) {
+    if (!host_buf || !gb_per_s) return set_error(Q1_ERR_INVALID_ARGUMENT, "null argument");
+    if (bytes < 4096 || threads < 1 || threads > 1024)
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "bytes must be >= 4096 and threads 1..1024");
+    *gb_per_s = host_read_gbs(host_buf, bytes, threads);
+    return Q1_OK;
+}
+
 q1_status q1_device_describe(int32_t device, char* buf, size_t buf_len) {
     if (!buf || !buf_len) return set_error(Q1_ERR_INVALID_ARGUMENT, "null buffer");
     cudaDeviceProp p;

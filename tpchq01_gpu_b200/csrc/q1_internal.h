@@ -138,5 +138,7 @@ bool cpu_aggregate_uncompressed(const HostUncompressed& t, uint64_t begin, uint6
                                 Agg128* out);
 // Bitmap words for rows [begin, end); begin must be a multiple of 32 (src/main.cu:367-368).
 void cpu_precompute_filter(const uint16_t* ship, uint64_t begin, uint64_t end, int32_t cutoff_rel, uint32_t* bitmap);
+// Rate at which `threads` host threads read [buf, buf + bytes), GB/s (q1_measure_host_read).
+double host_read_gbs(const void* buf, uint64_t bytes, int threads);
 
 }  // namespace q1
