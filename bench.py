@@ -307,6 +307,7 @@ def main():
     ap.add_argument("--placement", default="in_registers_per_thread")
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--pushdown", action="store_true", help="scan: read the predicate bitmap (filter pushdown)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="scan mode: leave out the batched-vs-plain (C3) object")
     ap.add_argument("--no-serve", action="store_true", help="scan mode: leave out the served-vs-plain (C4) object")
@@ -369,10 +370,15 @@ def main():
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
     launches = [0]
+    if args.pushdown:
+        # filter pushdown: the kernels read the predicate bitmap (1 bit/row) instead of ship dates
+        filt = torch.empty((rows + 31) // 32 + 8, dtype=torch.int32, device="cuda")
+        q.precompute_filter(comp.shipdate, rows, CUTOFF, filt.data_ptr(), sh)
+        comp.filter = filt.data_ptr()
 
     def step():
         aggs.zero_()
-        q.launch_compressed(args.placement, comp, rows, CUTOFF, False, aggs.data_ptr(), sh)
+        q.launch_compressed(args.placement, comp, rows, CUTOFF, args.pushdown, aggs.data_ptr(), sh)
         launches[0] += 1
 
     def exchange():
@@ -399,7 +405,7 @@ def main():
     for i in range(args.steps):
         aggs.zero_()
         ev[i][0].record(stream)
-        q.launch_compressed(args.placement, comp, rows, CUTOFF, False, aggs.data_ptr(), sh)
+        q.launch_compressed(args.placement, comp, rows, CUTOFF, args.pushdown, aggs.data_ptr(), sh)
         launches[0] += 1
         ev[i][1].record(stream)
         exchange()
@@ -420,16 +426,17 @@ def main():
 
     value = world * ROWS * args.steps / (total_ms / 1000.0)
     avg_kernel_s = sum(kern_ms) / len(kern_ms) / 1000.0
-    bytes_per_row = BYTES_PER_ROW if args.packing == "pair" else 9.375
+    bytes_per_row = (BYTES_PER_ROW if args.packing == "pair" else 9.375) - (1.875 if args.pushdown else 0.0)
     achieved = bytes_per_row * ROWS / avg_kernel_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic() if args.packing == "pair" else None
+    traffic = profiled_traffic() if args.packing == "pair" and not args.pushdown else None
 
     result = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
               "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
               "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
               "config": dict(config_dict(world, args.placement), **(
-                  {} if args.packing == "pair" else {"layout": "compressed 9.375 B/row (separate rf/ls containers)"})),
+                  {} if args.packing == "pair" else {"layout": "compressed 9.375 B/row (separate rf/ls containers)"}),
+                  **({"filter_pushdown": True, "bytes_per_row": bytes_per_row} if args.pushdown else {})),
               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                            "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} (hbm_gbs)",
                            "kernel_ms": sum(kern_ms) / len(kern_ms)},

@@ -36,7 +36,9 @@ typedef enum q1_status {
     Q1_ERR_OUT_OF_MEMORY    = 3,  /* device or pinned allocation failed                          */
     Q1_ERR_NOT_LOADED       = 4,  /* q1_run before q1_load_columns                              */
     Q1_ERR_UNSUPPORTED      = 5,  /* layout / placement combination not offered                 */
-    Q1_ERR_DOMAIN           = 6,  /* a value does not fit the compressed column types          */
+    Q1_ERR_DOMAIN           = 6,  /* a value does not fit the compressed column types, or a
+                                     reference-typed row's int64 products overflow (the
+                                     reference's handle_overflow)                              */
     Q1_ERR_DEVICE_TIMEOUT   = 7,  /* a bounded device-side wait expired; the context stays usable */
     Q1_ERR_BUSY             = 8,  /* serving: admission refused (slots or memory budget)         */
     Q1_ERR_CPU_WORKER       = 9,  /* a coprocessing CPU worker failed                            */
@@ -325,7 +327,11 @@ q1_status q1_launch_compressed_noalloc(q1_placement placement, const q1_compress
                                        const q1_launch_config* cfg, q1_i128* dev_aggregates,
                                        void* cuda_stream);
 
-/* Replaces the kernels table (src/main.cu:166-173): K1, K4, K7, K10, K13. */
+/* Replaces the kernels table (src/main.cu:166-173): K1, K4, K7, K10, K13. Takes any int64
+ * values, like the reference's CPU kernels: rows in the fast domain (discount 0..100, tax 0..255,
+ * quantity and price 0..2^32-1) are summed by the placement's tables, any other passing row
+ * exactly by a signed 128-bit path; a passing row whose int64 products overflow is reported as
+ * Q1_ERR_DOMAIN by q1_sync_check (KernelHyPer's handle_overflow, cpu/kernel_hyper.hpp:65-91). */
 q1_status q1_launch_uncompressed(q1_placement placement, const q1_columns* dev_cols,
                                  uint64_t rows, int32_t cutoff_day,
                                  const q1_launch_config* cfg, q1_i128* dev_aggregates,
@@ -650,7 +656,8 @@ q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream);
  * domain. Needs no GPU; for tests of the host kernel. */
 q1_status q1_selftest_cpu_share(const q1_compressed_columns* host_cols, uint64_t begin, uint64_t end,
                                 int32_t cutoff_day, void* aggregates);
-/* The same for reference-typed (uncompressed) columns in host memory. */
+/* The same for reference-typed (uncompressed) columns in host memory: any int64 values, summed
+ * exactly; Q1_ERR_DOMAIN when a passing row's int64 products overflow. */
 q1_status q1_selftest_cpu_share_uncompressed(const q1_columns* host_cols, uint64_t begin, uint64_t end,
                                              int32_t cutoff_day, void* aggregates);
 

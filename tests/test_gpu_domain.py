@@ -141,3 +141,52 @@ def test_default_grid_carries_past_2_64(cuda, maximal):
         q.launch_compressed("in_registers_per_thread", c, len(cols["shipdate"]), CUTOFF, False, buf.data_ptr(), stream)
     q.sync_check(stream)
     assert np.array_equal(read(buf), 3 * want)
+
+
+@pytest.fixture(scope="module")
+def wide_unc():
+    from test_host import wide_rows
+    return wide_rows(gen_np.generate(607, 0, ROWS), 607)
+
+
+@pytest.mark.parametrize("placement", PLACEMENTS)
+def test_uncompressed_wide_values_summed_exactly(cuda, wide_unc, placement):
+    """Reference-typed rows beyond the fast domain (negative or large int64 values whose products
+    still fit int64) are summed exactly, as the reference's KernelHyPer sums them."""
+    want, flag = O.q1_uncompressed(wide_unc, CUTOFF)
+    assert flag == 0
+    keep = {k: dev(v) for k, v in wide_unc.items()}
+    c = _lib.Columns(*[keep[k].data_ptr() for k in ["shipdate", "discount", "extendedprice", "tax", "quantity",
+                                                    "returnflag", "linestatus"]])
+    buf = aggs_buffer()
+    stream = torch.cuda.current_stream().cuda_stream
+    q.launch_uncompressed(placement, c, ROWS, CUTOFF, buf.data_ptr(), stream)
+    q.sync_check(stream)
+    assert np.array_equal(read(buf), want)
+
+
+@pytest.mark.parametrize("fraction", [0.0, 0.4])
+def test_uncompressed_wide_values_through_q1_run(cuda, wide_unc, fraction):
+    """The same rows through q1_run, GPU alone and with the CPU share of coprocessing."""
+    want, _ = O.q1_uncompressed(wide_unc, CUTOFF)
+    with q.Q1Context(cpu_threads=3) as ctx:
+        ctx.load_columns(wide_unc, "uncompressed", "pair", "hbm")
+        res = ctx.run(apply_compression=False, use_coprocessing=fraction > 0, cpu_processing_fraction=fraction,
+                      num_query_execution_runs=1)
+    assert np.array_equal(res.table(), want)
+
+
+def test_uncompressed_int64_overflow_is_reported(cuda):
+    """A passing row whose charge overflows int64 (the reference's handle_overflow) is reported."""
+    cols = {k: v.copy() for k, v in gen_np.generate(608, 0, 5000).items()}
+    i = int(np.argmax(cols["shipdate"] <= CUTOFF))
+    cols["extendedprice"][i] = 1 << 58
+    assert O.q1_uncompressed(cols, CUTOFF)[1] == 1
+    keep = {k: dev(v) for k, v in cols.items()}
+    c = _lib.Columns(*[keep[k].data_ptr() for k in ["shipdate", "discount", "extendedprice", "tax", "quantity",
+                                                    "returnflag", "linestatus"]])
+    stream = torch.cuda.current_stream().cuda_stream
+    q.launch_uncompressed("in_registers_per_thread", c, 5000, CUTOFF, aggs_buffer().data_ptr(), stream)
+    with pytest.raises(q.Q1Error) as e:
+        q.sync_check(stream)
+    assert e.value.status == 6

@@ -241,3 +241,55 @@ def test_cpu_share_uncompressed_equals_oracle(edges, cutoff):
     want, flag = O.q1_uncompressed(cols, cutoff)
     assert flag == 0
     assert np.array_equal(O.i128_to_ints(buf, 6), want)
+
+
+def wide_rows(cols, seed, frac=0.03):
+    """Replaces `frac` of the rows by reference-typed values beyond the fast domain that the
+    reference's int64 arithmetic still takes without overflow: prices up to 2^40 and quantities up
+    to 2^44 (both also negative), negative and above-100 discounts, taxes up to 1023 and negative
+    ones; |(100 - d) p (100 + t)| stays below 2^63."""
+    rng = np.random.default_rng(seed)
+    n = len(cols["shipdate"])
+    idx = rng.choice(n, int(frac * n), replace=False)
+    k = len(idx)
+    out = {key: np.ascontiguousarray(v).copy() for key, v in cols.items()}
+    out["extendedprice"][idx] = rng.integers(-(1 << 40), 1 << 40, k)
+    out["quantity"][idx] = rng.integers(-(1 << 40), 1 << 44, k)
+    out["discount"][idx] = rng.integers(-4000, 4000, k)
+    out["tax"][idx] = rng.integers(-1000, 1024, k)
+    return out
+
+
+def cpu_share_unc(cols, cutoff, ranges):
+    cc = _lib.Columns()
+    for k in ["shipdate", "discount", "extendedprice", "tax", "quantity", "returnflag", "linestatus"]:
+        setattr(cc, k, cols[k].ctypes.data)
+    buf = np.zeros(6 * 6 * 2, dtype=np.uint64)
+    st = 0
+    for b, e in ranges:
+        st |= q.lib().q1_selftest_cpu_share_uncompressed(ctypes.byref(cc), b, e, cutoff, ctypes.c_void_p(buf.ctypes.data))
+    return O.i128_to_ints(buf, 6), st
+
+
+@pytest.mark.parametrize("cutoff", [728000, 729999])
+def test_cpu_share_uncompressed_wide_values_equal_oracle(cutoff):
+    """Reference-typed rows outside the kernels' fast domain are summed exactly (signed 128-bit),
+    like the reference's KernelHyPer sums any int64 values whose products do not overflow."""
+    rows = 100_003
+    cols = wide_rows(gen_np.generate(45, 0, rows), cutoff)
+    got, st = cpu_share_unc(cols, cutoff, [(0, 13), (13, 60_001), (60_001, rows)])
+    want, flag = O.q1_uncompressed(cols, cutoff)
+    assert flag == 0 and st == 0
+    assert np.array_equal(got, want)
+    assert min(int(want[g, 4]) for g in range(6)) < 0   # negative disc_price sums occur
+
+
+def test_cpu_share_uncompressed_reports_int64_overflow():
+    """A passing row whose charge overflows int64 (the reference's handle_overflow) is reported as
+    Q1_ERR_DOMAIN, as the oracle flags it."""
+    cols = {k: np.ascontiguousarray(v).copy() for k, v in gen_np.generate(46, 0, 1000).items()}
+    i = int(np.argmax(cols["shipdate"] <= 729999))
+    cols["extendedprice"][i] = 1 << 58
+    got, st = cpu_share_unc(cols, 729999, [(0, 1000)])
+    _, flag = O.q1_uncompressed(cols, 729999)
+    assert flag == 1 and st == 6

@@ -9,13 +9,18 @@
 // process exits:
 //   words [0, 32)                 status block (word 0 = the kernel status bits)
 //   words [32, 32 + 256 * 72)     one record per CTA: 6 groups x 6 aggregates x (lo, hi)
-// The scan kernel writes its CTA's partial sums into its record (instead of atomics into the
-// caller's table) and a one-block reduction kernel adds the records into the caller's table.
+// In the placements with per-thread or per-lane tables (in_registers, in_registers_per_thread,
+// local_mem, shared_mem_per_thread) the scan kernel writes its CTA's partial sums into its record
+// instead of one 128-bit atomic per (group, aggregate) into the caller's table, and a one-block
+// reduction kernel adds the records into the caller's table. The global placement keeps no CTA
+// partials: its warps add every tile's sums straight into the caller's table, as they do under
+// q1_launch_compressed, so its records stay zero and the reduction adds nothing.
 // Limit: at most kNoAllocMaxCtas CTAs per launch (the library uses one per SM, 148 on a B200).
 //
 // The array is shared by every call and keeps the last call's contents: each call clears the
 // status word before launching, and every CTA overwrites its whole record. Calls whose GPU work
 // overlaps (two host threads, or two streams of one device) race on this array.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -38,20 +43,61 @@ constexpr uint32_t kNoAllocWords = kNoAllocStatusWords + kNoAllocMaxCtas * kReco
 
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocWords];   // 147,712 bytes
 
-// Device address of g_noalloc_scratch per device, resolved once with that device current.
+// Device address of g_noalloc_scratch per device, resolved with that device current by the
+// first call on the device, and again by the first call after the device's context was replaced
+// (cudaDeviceReset destroys the context and the module with the array; the next context loads it
+// again, possibly at another address). A context is told apart by the unique id the driver gives
+// every context (cuCtxGetId), reached through the runtime's driver entry points so that the
+// library needs no link against the driver library.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+struct NoAllocSlot {
+    unsigned long long ctx_id = 0;
+    unsigned long long* ptr = nullptr;
+};
+
 static std::mutex g_noalloc_mutex;
-static unsigned long long* g_noalloc_ptr[64] = {};
+static NoAllocSlot g_noalloc_slot[64];
+static CtxGetCurrentFn g_ctx_get_current = nullptr;
+static CtxGetIdFn g_ctx_get_id = nullptr;
+
+static q1_status current_context_id(unsigned long long* id) {
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult found;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &found);
+        if (e != cudaSuccess || found != cudaDriverEntryPointSuccess || !f)
+            return set_error(Q1_ERR_CUDA, "driver entry point cuCtxGetCurrent not found");
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &found);
+        if (e != cudaSuccess || found != cudaDriverEntryPointSuccess || !f)
+            return set_error(Q1_ERR_CUDA, "driver entry point cuCtxGetId not found");
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return set_error(Q1_ERR_CUDA, "no current CUDA context");
+    if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return set_error(Q1_ERR_CUDA, "cuCtxGetId failed");
+    return Q1_OK;
+}
 
 static q1_status noalloc_scratch(int device, unsigned long long** out) {
     if (device < 0 || device >= 64) return set_error(Q1_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_noalloc_mutex);
-    if (!g_noalloc_ptr[device]) {
+    // Makes the device's primary context current, creating it if a reset destroyed it.
+    Q1_CUDA(cudaSetDevice(device));
+    unsigned long long id = 0;
+    q1_status st = current_context_id(&id);
+    if (st != Q1_OK) return st;
+    NoAllocSlot& slot = g_noalloc_slot[device];
+    if (!slot.ptr || slot.ctx_id != id) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_noalloc_ptr[device] = static_cast<unsigned long long*>(p);
+        slot.ptr = static_cast<unsigned long long*>(p);
+        slot.ctx_id = id;
     }
-    *out = g_noalloc_ptr[device];
+    *out = slot.ptr;
     return Q1_OK;
 }
 

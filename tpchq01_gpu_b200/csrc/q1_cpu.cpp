@@ -187,6 +187,26 @@ struct Partial {
     }
 };
 
+// A passing reference-typed row outside the fast domain (any int64 values), with the reference's
+// arithmetic (cpu/kernel_hyper.hpp:70-83) in exact signed 128-bit sums, as the GPU kernels' wide
+// path does. Returns false, adding nothing, when an int64 product or difference of the reference
+// would overflow (its handle_overflow).
+inline bool wide_row(Agg128* out, uint32_t g, int64_t q, int64_t d, int64_t t, int64_t pr) {
+    const __int128 d1 = (__int128)100 - d, t1 = (__int128)100 + t;
+    const __int128 dp = d1 * pr;
+    const __int128 ch = dp * t1;
+    const auto fits = [](__int128 v) { return v >= (__int128)INT64_MIN && v <= (__int128)INT64_MAX; };
+    if (!fits(d1) || !fits(t1) || !fits(dp) || !fits(ch)) return false;
+    u128* o = out->v[g];
+    o[kAggCount] += 1;
+    o[kAggQty] += (u128)(__int128)q;
+    o[kAggBasePrice] += (u128)(__int128)pr;
+    o[kAggDisc] += (u128)(__int128)d;
+    o[kAggDiscPrice] += (u128)dp;
+    o[kAggCharge] += (u128)ch;
+    return true;
+}
+
 inline void add_row(Partial& p, uint32_t g, uint64_t q, uint64_t d, uint64_t t, uint64_t pr) {
     const uint64_t a = 100 - d;
     const uint64_t dp = a * pr;
@@ -511,11 +531,21 @@ __attribute__((target("avx512f,avx512bw,avx512dq,avx512vl"))) bool aggregate_unc
             for (int k = 0; k < 4; ++k) acc[g][k] = _mm512_setzero_si512();
         __mmask8 bad = 0;
         for (uint64_t i = b0; i < b1; i += 8) {
-            const __mmask8 pass = _mm256_cmple_epi32_mask(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(t.ship + i)), cut);
+            const __mmask8 pass_all =
+                _mm256_cmple_epi32_mask(_mm256_loadu_si256(reinterpret_cast<const __m256i*>(t.ship + i)), cut);
             const __m512i Q = _mm512_loadu_si512(t.qty + i), D = _mm512_loadu_si512(t.disc + i);
             const __m512i X = _mm512_loadu_si512(t.tax + i), P = _mm512_loadu_si512(t.price + i);
-            bad |= _mm512_mask_cmpgt_epu64_mask(pass, Q, max32) | _mm512_mask_cmpgt_epu64_mask(pass, D, hundred) |
-                   _mm512_mask_cmpgt_epu64_mask(pass, X, max8) | _mm512_mask_cmpgt_epu64_mask(pass, P, max32);
+            // passing rows outside the fast domain (unsigned compares also catch negative values)
+            const __mmask8 wide = _mm512_mask_cmpgt_epu64_mask(pass_all, Q, max32) |
+                                  _mm512_mask_cmpgt_epu64_mask(pass_all, D, hundred) |
+                                  _mm512_mask_cmpgt_epu64_mask(pass_all, X, max8) |
+                                  _mm512_mask_cmpgt_epu64_mask(pass_all, P, max32);
+            for (uint32_t w = wide; w; w &= w - 1) {
+                const uint64_t j = i + (uint64_t)__builtin_ctz(w);
+                bad |= !wide_row(out, group_of(encode_return_flag(t.rf[j]), encode_line_status(t.ls[j])), t.qty[j],
+                                 t.disc[j], t.tax[j], t.price[j]);
+            }
+            const __mmask8 pass = (__mmask8)(pass_all & ~wide);
             const __m512i DP = _mm512_mullo_epi64(_mm512_sub_epi64(hundred, D), P);
             const __m512i CH = _mm512_mullo_epi64(DP, _mm512_add_epi64(hundred, X));
             const __m512i QC = _mm512_add_epi64(Q, cnt1);
@@ -577,9 +607,11 @@ bool cpu_aggregate_uncompressed(const HostUncompressed& t, uint64_t begin, uint6
         for (uint64_t i = b0; i < b1; ++i) {
             if (t.ship[i] > cutoff_day) continue;
             const int64_t q = t.qty[i], d = t.disc[i], x = t.tax[i], p = t.price[i];
-            ok &= (q >= 0 && q < (1ll << 32) && d >= 0 && d <= 100 && x >= 0 && x <= 255 && p >= 0 && p < (1ll << 32));
             const uint32_t g = group_of(encode_return_flag(t.rf[i]), encode_line_status(t.ls[i]));
-            add_row(part, g, (uint64_t)q, (uint64_t)d, (uint64_t)x, (uint64_t)p);
+            if (q >= 0 && q < (1ll << 32) && d >= 0 && d <= 100 && x >= 0 && x <= 255 && p >= 0 && p < (1ll << 32))
+                add_row(part, g, (uint64_t)q, (uint64_t)d, (uint64_t)x, (uint64_t)p);
+            else
+                ok &= wide_row(out, g, q, d, x, p);
         }
         part.into(out);
     }

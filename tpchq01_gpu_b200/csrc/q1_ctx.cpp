@@ -836,7 +836,8 @@ static q1_status run_once(q1_ctx* ctx, const q1_params* prm, Agg128* total, doub
         ctx->queue.close();
         if (!ctx->pool->wait() && st == Q1_OK) st = set_error(Q1_ERR_CPU_WORKER, "CPU worker failed: " + ctx->pool->error());
         if (cpu_domain_bad.load() && st == Q1_OK)
-            st = set_error(Q1_ERR_DOMAIN, "a row of the CPU share is outside the kernel domain");
+            st = set_error(Q1_ERR_DOMAIN, "a row of the CPU share is outside the kernels' domain (compressed) or "
+                                          "its int64 products overflow (reference-typed)");
     }
     if (st != Q1_OK) {
         // leave every stream idle before reporting

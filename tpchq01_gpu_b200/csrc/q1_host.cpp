@@ -86,8 +86,9 @@ q1_status check_device_status(cudaStream_t stream, uint32_t* status_word) {
         Q1_CUDA(cudaMemset(status_word, 0, sizeof(bits)));
         if (bits & 1u) return set_error(Q1_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
         if (bits & 4u) return set_error(Q1_ERR_INTERNAL, "a device work buffer would have overflowed");
-        return set_error(Q1_ERR_DOMAIN, "a row is outside the kernel domain (discount > 100, tax > 255, "
-                                        "or a value >= 2^32 / negative)");
+        return set_error(Q1_ERR_DOMAIN, "a row is outside the kernels' domain: a compressed row with a discount "
+                                        "above 100 or a ship offset above 32767, or a reference-typed row whose "
+                                        "int64 products overflow");
     }
     return Q1_OK;
 }
@@ -695,7 +696,7 @@ q1_status q1_selftest_cpu_share_uncompressed(const q1_columns* cols, uint64_t be
     memcpy(&a, aggregates, sizeof(a));
     const bool ok = cpu_aggregate_uncompressed(h, begin, end, cutoff_day, &a);
     memcpy(aggregates, &a, sizeof(a));
-    return ok ? Q1_OK : set_error(Q1_ERR_DOMAIN, "a passing row is outside the kernels' domain");
+    return ok ? Q1_OK : set_error(Q1_ERR_DOMAIN, "a passing row's int64 products overflow");
 }
 
 q1_status q1_selftest_wait_timeout(uint32_t limit_us, void* cuda_stream) {

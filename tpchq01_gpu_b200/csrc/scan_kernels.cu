@@ -18,10 +18,15 @@
 // Every wait is bounded (q1_ptx.cuh, kWaitLimitNs); on expiry the kernel records
 // kStatusWaitTimeout in the status word, drains its own copies and returns.
 //
-// Domain: discount <= 100 (so 100 - d >= 0), tax <= 255, extendedprice and quantity < 2^32.
+// Fast domain: discount <= 100 (so 100 - d >= 0), tax <= 255, extendedprice and quantity < 2^32.
 // Then every per-row product fits 64 bits unsigned (charge < 2^47.2) and per-thread 64-bit
 // partials cannot wrap for launches of up to 2^31 rows (the host splits longer launches).
-// A row outside the domain sets kStatusDomain (the host reports Q1_ERR_DOMAIN).
+// Compressed columns cannot leave it except by a discount above 100 or a ship offset above 32767,
+// which set kStatusDomain (the host reports Q1_ERR_DOMAIN). The reference-typed (uncompressed)
+// columns are int64: a passing row outside the fast domain is summed exactly by wide_row (signed
+// 128-bit arithmetic, 128-bit atomics straight into the output), and only a row whose int64
+// products overflow, which the reference's KernelHyPer reports through handle_overflow
+// (cpu/kernel_hyper.hpp:65-91), sets kStatusDomain.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -282,6 +287,8 @@ struct AccPerThread {
         if constexpr (kWideQty) g[i].zero();
         else gq[i].zero();
     }
+    // whether this thread sums the rows of group code c (every thread reads every row it is given)
+    __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
@@ -329,6 +336,8 @@ struct AccWarpLane {
     }
     __device__ __forceinline__ void add_quad(const Quad& x) { rq.add_quad((x.OH >> my) & 0x01010101u, x); }
     __device__ __forceinline__ void fold() { r.fold(); }
+    // all G lanes of a table read the same rows; the lane of group c sums them
+    __device__ __forceinline__ bool owns(uint32_t c) const { return c == my; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
@@ -368,6 +377,8 @@ struct AccLocal {
             add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
     }
     __device__ __forceinline__ void fold() {}
+    // whether this thread sums the rows of group code c (every thread reads every row it is given)
+    __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
@@ -418,6 +429,8 @@ struct AccSharedPerThread {
             add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
     }
     __device__ __forceinline__ void fold() {}
+    // whether this thread sums the rows of group code c (every thread reads every row it is given)
+    __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
@@ -450,6 +463,7 @@ struct AccGlobal {
     }
     __device__ __forceinline__ void add_quad(const Quad& x) { buf.add_quad(x); }
     __device__ __forceinline__ void fold() { buf.fold(); }
+    __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P& prm, uint32_t lane) {
         buf.fold();
@@ -486,10 +500,39 @@ __device__ __forceinline__ uint32_t code_of_chars(uint32_t rf, uint32_t ls) {
     return (r << 1) + (ls == 'F' ? 0u : 1u);
 }
 
+__device__ __forceinline__ bool fits_i64(__int128 v) { return v >= (__int128)INT64_MIN && v <= (__int128)INT64_MAX; }
+
+__device__ __forceinline__ void atomic_add_i128(unsigned long long* p, __int128 v) {
+    atomic_add_u128(p, (uint64_t)(unsigned __int128)v, (uint64_t)((unsigned __int128)v >> 64));
+}
+
+// One passing reference-typed row outside the fast domain, summed exactly with the reference's
+// arithmetic (cpu/kernel_hyper.hpp:70-83): disc_1 = 100 - disc, tax_1 = 100 + tax,
+// disc_price = disc_1 * price, charge = disc_price * tax_1, each an int64 in the reference and
+// checked for overflow there; the six sums go straight into the output table as signed 128-bit
+// values. A row whose int64 arithmetic would overflow is reported instead of summed.
+__device__ __noinline__ void wide_row(const ScanParams& prm, uint32_t group, int64_t q, int64_t d, int64_t t,
+                                      int64_t p) {
+    const __int128 d1 = (__int128)100 - d, t1 = (__int128)100 + t;
+    const __int128 dp = d1 * p;
+    const __int128 ch = dp * t1;   // |dp| < 2^64 and |t1| < 2^64 here, so the product is exact
+    if (!fits_i64(d1) || !fits_i64(t1) || !fits_i64(dp) || !fits_i64(ch)) {
+        if (prm.status) atomicOr(prm.status, kStatusDomain);
+        return;
+    }
+    unsigned long long* o = prm.out + 2 * (group * kNumAggs);
+    atomic_add_i128(o + 2 * kAggCount, 1);
+    atomic_add_i128(o + 2 * kAggQty, (__int128)q * prm.qty_scale);
+    atomic_add_i128(o + 2 * kAggBasePrice, p);
+    atomic_add_i128(o + 2 * kAggDisc, d);
+    atomic_add_i128(o + 2 * kAggDiscPrice, dp);
+    atomic_add_i128(o + 2 * kAggCharge, ch);
+}
+
 // One step of rows [kRowsPerStep * j, +kRowsPerStep) of the tile held at shared address `base`.
 template <int L, class Acc>
-__device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t cut, uint32_t lut, Acc& acc,
-                                             uint32_t& bad) {
+__device__ __forceinline__ void process_step(const ScanParams& prm, uint32_t base, uint32_t j, int32_t cut,
+                                             uint32_t lut, Acc& acc, uint32_t& bad) {
     using T = LayoutTraits<L>;
     constexpr uint32_t R = kTileRows<L>;
     if constexpr (L == kLayUncomp) {
@@ -500,17 +543,21 @@ __device__ __forceinline__ void process_step(uint32_t base, uint32_t j, int32_t 
         const uint4 P = lds_v4(base + col_offset<L>(4, R) + 16 * j);
         const uint32_t RF = lds_u16(base + col_offset<L>(5, R) + 2 * j);
         const uint32_t LS = lds_u16(base + col_offset<L>(6, R) + 2 * j);
-        bad |= Q.y | Q.w | D.y | D.w | X.y | X.w | P.y | P.w;
-        bad |= (D.x > 100u) | (D.z > 100u) | (X.x > 255u) | (X.z > 255u);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const int32_t ship = (int32_t)(r ? sd.y : sd.x);
             const uint32_t code = code_of_chars((RF >> (8 * r)) & 0xFFu, (LS >> (8 * r)) & 0xFFu);
-            const uint32_t c = ship <= cut ? code : 7u;
             const uint32_t q = r ? Q.z : Q.x;
             const uint32_t d = r ? D.z : D.x;
             const uint32_t t = r ? X.z : X.x;
             const uint32_t p = r ? P.z : P.x;
+            const bool wide = ((r ? (Q.w | D.w | X.w | P.w) : (Q.y | D.y | X.y | P.y)) != 0u) | (d > 100u) | (t > 255u);
+            const bool pass = ship <= cut;
+            if (wide && pass && acc.owns(code))
+                wide_row(prm, code, (int64_t)((uint64_t)(r ? Q.w : Q.y) << 32 | q),
+                         (int64_t)((uint64_t)(r ? D.w : D.y) << 32 | d), (int64_t)((uint64_t)(r ? X.w : X.y) << 32 | t),
+                         (int64_t)((uint64_t)(r ? P.w : P.y) << 32 | p));
+            const uint32_t c = (pass && !wide) ? code : 7u;
             const uint32_t a = 100u - d;
             acc.add(c, q, d, a, a * (100u + t), p);
         }
@@ -560,8 +607,11 @@ __device__ __forceinline__ void process_row_global(const ScanParams& prm, uint64
         const uint64_t p = __ldg(reinterpret_cast<const unsigned long long*>(prm.col[4]) + i);
         const uint32_t rf = (uint8_t)__ldg(reinterpret_cast<const char*>(prm.col[5]) + i);
         const uint32_t ls = (uint8_t)__ldg(reinterpret_cast<const char*>(prm.col[6]) + i);
-        bad |= (uint32_t)((q | p) >> 32) | (d > 100u) | (t > 255u);
-        const uint32_t c = ship <= prm.cutoff ? code_of_chars(rf, ls) : 7u;
+        const bool wide = ((q | p) >> 32) != 0 || d > 100u || t > 255u;
+        const bool pass = ship <= prm.cutoff;
+        if (wide && pass && acc.owns(code_of_chars(rf, ls)))
+            wide_row(prm, code_of_chars(rf, ls), (int64_t)q, (int64_t)d, (int64_t)t, (int64_t)p);
+        const uint32_t c = (pass && !wide) ? code_of_chars(rf, ls) : 7u;
         const uint32_t a = 100u - (uint32_t)d;
         acc.add(c, (uint32_t)q, (uint32_t)d, a, a * (100u + (uint32_t)t), (uint32_t)p);
     } else {
@@ -691,12 +741,12 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
                 const uint32_t tbl = lane / G;
                 if (tbl < kTablesPerWarp) {
                     for (uint32_t j = warp * kTablesPerWarp + tbl; j < kSteps; j += W * kTablesPerWarp)
-                        process_step<L>(base, j, prm.cutoff, lut, acc, bad);
+                        process_step<L>(prm, base, j, prm.cutoff, lut, acc, bad);
                 }
             } else {
 #pragma unroll
                 for (uint32_t it = 0; it < kSteps / (W * 32); ++it)
-                    process_step<L>(base, ctid + it * (W * 32), prm.cutoff, lut, acc, bad);
+                    process_step<L>(prm, base, ctid + it * (W * 32), prm.cutoff, lut, acc, bad);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
