@@ -569,9 +569,10 @@ typedef enum q1_serve_mode {
 
 typedef struct q1_server_opts {
     int32_t  device;
-    uint32_t max_inflight;       /* requests per round (response slots) */
+    uint32_t max_inflight;       /* requests per round (response slots of a round lane) */
     int32_t  mode;               /* q1_serve_mode */
-    uint32_t reserved;
+    uint32_t max_rounds_in_flight;  /* round lanes: rounds on the GPU at once, 1..8 (0 = 2);
+                                       Q1_SERVE_PLAIN always runs one */
     uint64_t seed;               /* resident table seed */
     uint64_t resident_rows;      /* rows of the resident table */
     uint64_t hbm_budget_bytes;   /* arena of resident ad-hoc tables (13 B per row + alignment) */
@@ -591,6 +592,9 @@ typedef struct q1_server_stats {
     double   wall_ms;            /* first completed request's submission -> last completion */
     double   mean_round_size;
     double   p50_ms, p90_ms, p99_ms, max_ms, mean_ms;   /* latency of completed requests */
+    uint64_t overlapped_rounds;  /* rounds enqueued while another round was on the GPU */
+    uint32_t max_rounds_in_flight;  /* most rounds on the GPU at once */
+    uint32_t reserved;
 } q1_server_stats;
 
 typedef struct q1_server q1_server;

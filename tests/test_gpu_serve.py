@@ -24,10 +24,11 @@ RES, ADHOC = _lib.REQ_RESIDENT, _lib.REQ_ADHOC
 EDGE_CUTOFFS = [700000, 727562, 727563, 727564, 728826, 729999, 730089, 740000]
 
 
-def open_server(budget=256 << 20, slots=16, mode=_lib.SERVE_BATCHED):
+def open_server(budget=256 << 20, slots=16, mode=_lib.SERVE_BATCHED, lanes=0):
     o = _lib.ServerOpts()
     q.lib().q1_server_opts_default(ctypes.byref(o))
     o.mode = mode
+    o.max_rounds_in_flight = lanes
     o.seed = SEED
     o.resident_rows = RES_ROWS
     o.hbm_budget_bytes = budget
@@ -238,5 +239,42 @@ def test_budget_refusal(cuda):
         small = req(ADHOC, KEYS, 729999, 3, 10_000, 5)
         got = wait(h, submit(h, small))
         assert np.array_equal(words(got), words(plain(h, small)))
+    finally:
+        _lib.check(q.lib().q1_server_close(h))
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4])
+def test_rounds_overlap_on_the_device(cuda, lanes):
+    """Continuous batching: a burst larger than one round's slots forms round after round, and with
+    more than one round lane a round is enqueued while the previous one is still on the GPU (its
+    copies and kernels queue behind it on another stream). Every response equals the plain path."""
+    h = open_server(slots=4, lanes=lanes)
+    try:
+        rng = np.random.default_rng(lanes)
+        reqs = []
+        for i in range(40):
+            rows = int(rng.integers(200_000, ADHOC_MAX))
+            if i % 5 == 0:
+                reqs.append(req(RES, FLAGS if i % 2 else KEYS, int(rng.integers(729906, 730090)), 0 if i % 2 else 64))
+            else:
+                reqs.append(req(ADHOC, KEYS if i % 3 else FLAGS, int(rng.integers(729906, 730090)),
+                                [4, 9, 64][i % 3] if i % 3 else 0, rows, 500 + i % 7))
+        # make the tables resident first, so that the burst below is all scans
+        for r in reqs:
+            if r.kind == ADHOC:
+                wait(h, submit(h, r))
+        _lib.check(q.lib().q1_server_reset_stats(h))
+        tickets = [submit(h, r) for r in reqs]
+        got = [words(wait(h, t)) for t in tickets]
+        st = _lib.ServerStats()
+        _lib.check(q.lib().q1_server_stats_get(h, ctypes.byref(st)))
+        assert st.completed == len(reqs) and st.failed == 0 and st.rounds >= len(reqs) // 4
+        assert st.max_rounds_in_flight <= lanes
+        if lanes == 1:
+            assert st.overlapped_rounds == 0
+        else:
+            assert st.overlapped_rounds > 0 and st.max_rounds_in_flight >= 2
+        for r, g in zip(reqs, got):
+            assert np.array_equal(g, words(plain(h, r)))
     finally:
         _lib.check(q.lib().q1_server_close(h))

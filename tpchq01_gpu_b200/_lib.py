@@ -141,7 +141,7 @@ class Response(ctypes.Structure):
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_inflight", ctypes.c_uint32), ("mode", ctypes.c_int32),
-                ("reserved", ctypes.c_uint32), ("seed", ctypes.c_uint64),
+                ("max_rounds_in_flight", ctypes.c_uint32), ("seed", ctypes.c_uint64),
                 ("resident_rows", ctypes.c_uint64), ("hbm_budget_bytes", ctypes.c_uint64),
                 ("max_adhoc_rows", ctypes.c_uint64)]
 
@@ -153,7 +153,8 @@ class ServerStats(ctypes.Structure):
                 ("evictions", ctypes.c_uint64), ("cached_tables", ctypes.c_uint64), ("cached_bytes", ctypes.c_uint64),
                 ("wall_ms", ctypes.c_double), ("mean_round_size", ctypes.c_double), ("p50_ms", ctypes.c_double),
                 ("p90_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
-                ("mean_ms", ctypes.c_double)]
+                ("mean_ms", ctypes.c_double), ("overlapped_rounds", ctypes.c_uint64),
+                ("max_rounds_in_flight", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/q1.h

@@ -11,13 +11,21 @@
 // resident; when a new table does not fit, least recently used tables that no admitted request
 // reads are evicted.
 //
-// A dispatcher thread forms a round from the queue head (FIFO) as long as a response slot is
-// free and, for an ad-hoc request, its table is or can be made resident; requests that arrive
-// while a round is on the GPU join the next one. A round = generate the missing tables, one
-// launch of the persistent batch kernel over all ad-hoc requests (batch_kernels.cu), one lookup
-// kernel for the resident requests, one copy of every response back to the host. Latency is
-// measured per request from submission to completion. Q1_SERVE_PLAIN runs the same loop with
-// one request per round and one plain scan launch per request: the comparison point.
+// Continuous batching over round lanes. A lane is one round's worth of streams, device and pinned
+// buffers and a status word (opts.max_rounds_in_flight lanes, 2 by default). A dispatcher thread
+// forms a round from the queue head (FIFO) whenever a lane is free, as long as a response slot is
+// free and, for an ad-hoc request, its table is or can be made resident, and enqueues it on the
+// lane's streams without waiting: requests that arrive while a round is on the GPU form the next
+// round at once, and its copies, generation and kernels queue behind and overlap the running
+// round on the device (the persistent kernels of the next round take SMs as the running round's
+// CTAs finish). A completer thread retires rounds in order: it waits for the oldest lane's
+// streams, reads the lane's status word and the responses, completes the tickets and frees the
+// lane. A round = generate the missing tables, one launch of the persistent batch kernel over all
+// ad-hoc requests (batch_kernels.cu), one lookup kernel for the resident requests, one copy of
+// every response back to the host. A table generated by one lane and read by another is ordered
+// by an event. Latency is measured per request from submission to completion. Q1_SERVE_PLAIN
+// runs the same loop with one lane, one request per round and one plain scan launch per request:
+// the comparison point.
 //
 // q1_server_plain answers one request from scratch (fresh table, plain scan launch) on its own
 // stream and is the arbiter every served response must equal bit for bit.
@@ -173,7 +181,9 @@ struct CachedTable {
     uint64_t off = 0, len = 0;
     uint32_t pins = 0;        // requests of the forming or running round that read it
     uint64_t last_use = 0;
-    bool ready = false;       // generated (in stream order before any reader)
+    bool ready = false;       // generation enqueued (readers on other lanes wait for gen_ev)
+    cudaEvent_t gen_ev = nullptr;   // recorded after the generation on gen_stream
+    cudaStream_t gen_stream = nullptr;
 };
 
 struct Ticket {
@@ -228,13 +238,43 @@ inline int32_t cutoff_rel(int32_t cutoff_day) {
 
 }  // namespace
 
+namespace {
+
+// One round in flight: its streams (the round; the batch's register-planes kernel), device and
+// pinned buffers and status word, and the tickets it answers.
+struct Lane {
+    cudaStream_t stream = nullptr, aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    Dev d_resp, d_inst, d_items, d_base, d_scratch, d_cursor, d_lookup, d_status;
+    Pinned h_resp, h_inst, h_items, h_base, h_lookup, h_status;
+    uint64_t items_cap = 0;
+    std::vector<Ticket*> batch;
+    q1_status enq = Q1_OK;   // status of enqueueing the round
+    std::string err;
+    Lane() = default;
+    Lane(const Lane&) = delete;
+    Lane& operator=(const Lane&) = delete;
+    ~Lane() {
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+        if (aux) {
+            cudaStreamSynchronize(aux);
+            cudaStreamDestroy(aux);
+        }
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+    }
+};
+
+}  // namespace
+
 struct q1_server {
     int device = 0;
     DeviceInfo* di = nullptr;
-    cudaStream_t stream = nullptr;         // rounds
+    cudaStream_t stream = nullptr;         // building the resident table at open
     cudaStream_t plain_stream = nullptr;   // q1_server_plain
-    cudaStream_t aux = nullptr;            // the batch's register-planes kernel
-    cudaEvent_t fork = nullptr, join = nullptr;
     q1_server_opts opts{};
 
     // resident table: ship | qty | disc | tax | price | codes | keys
@@ -251,10 +291,9 @@ struct q1_server {
     std::map<TableKey, CachedTable> cache;
     uint64_t lru_clock = 0;
 
-    // rounds
-    Dev d_resp, d_inst, d_items, d_base, d_scratch, d_cursor, d_lookup;
-    Pinned h_resp, h_inst, h_items, h_base, h_lookup;
-    uint64_t items_cap = 0;
+    // round lanes: free ones, and the ones whose round is on the GPU in submission order
+    std::vector<std::unique_ptr<Lane>> lanes;
+    std::deque<Lane*> free_lanes, inflight;
 
     // plain launches: plain_scratch for Q1_SERVE_PLAIN rounds (dispatcher thread); the arbiter
     // (q1_server_plain) has buffers of its own, serialised by arbiter_m
@@ -264,12 +303,13 @@ struct q1_server {
 
     // queue
     std::mutex m;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_retire;
     std::deque<Ticket*> pending;
     std::unordered_map<uint64_t, std::unique_ptr<Ticket>> tickets;
     uint64_t next_id = 1;
     bool stop = false;
-    std::thread dispatcher;
+    bool dispatcher_done = false;
+    std::thread dispatcher, completer;
     q1_status fatal = Q1_OK;
     std::string fatal_msg;
 
@@ -277,6 +317,8 @@ struct q1_server {
     std::vector<double> latencies;
     uint64_t rounds = 0, completed = 0, failed = 0, logical_rows = 0, scanned_rows = 0, admitted_total = 0;
     uint64_t generated_rows = 0, cache_hits = 0, cache_misses = 0, evictions = 0;
+    uint64_t overlapped_rounds = 0;   // rounds enqueued while another round was on the GPU
+    uint32_t max_in_flight = 0;       // most rounds on the GPU at once
     double t_first = 0, t_last = 0;
 };
 
@@ -357,13 +399,36 @@ void complete(q1_server* s, Ticket* t, q1_status st, double when) {
     s->t_last = std::max(s->t_last, when);
 }
 
-q1_status grow_items(q1_server* s, uint64_t n) {
-    if (n <= s->items_cap) return Q1_OK;
+q1_status grow_items(Lane* L, uint64_t n) {
+    if (n <= L->items_cap) return Q1_OK;
     q1_status st;
-    if ((st = s->d_items.alloc(sizeof(BatchItem) * n)) != Q1_OK) return st;
-    if ((st = s->h_items.alloc(sizeof(BatchItem) * n)) != Q1_OK) return st;
-    s->items_cap = n;
+    if ((st = L->d_items.alloc(sizeof(BatchItem) * n)) != Q1_OK) return st;
+    if ((st = L->h_items.alloc(sizeof(BatchItem) * n)) != Q1_OK) return st;
+    L->items_cap = n;
     return Q1_OK;
+}
+
+q1_status lane_open(Lane* L, uint64_t m) {
+    Q1_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
+    Q1_CUDA(cudaStreamCreateWithFlags(&L->aux, cudaStreamNonBlocking));
+    Q1_CUDA(cudaEventCreateWithFlags(&L->fork, cudaEventDisableTiming));
+    Q1_CUDA(cudaEventCreateWithFlags(&L->join, cudaEventDisableTiming));
+    q1_status st;
+    if ((st = L->d_resp.alloc(m * kRespWords * 8)) != Q1_OK) return st;
+    if ((st = L->h_resp.alloc(m * kRespWords * 8)) != Q1_OK) return st;
+    if ((st = L->d_inst.alloc(sizeof(BatchInstanceDev) * m)) != Q1_OK) return st;
+    if ((st = L->h_inst.alloc(sizeof(BatchInstanceDev) * m)) != Q1_OK) return st;
+    if ((st = L->d_base.alloc(sizeof(uint64_t) * (m + 1))) != Q1_OK) return st;
+    if ((st = L->h_base.alloc(sizeof(uint64_t) * (m + 1))) != Q1_OK) return st;
+    if ((st = L->d_scratch.alloc(m * kMaxGroups * 64)) != Q1_OK) return st;
+    if ((st = L->d_cursor.alloc(4 * kEngines)) != Q1_OK) return st;
+    if ((st = L->d_lookup.alloc(sizeof(CubeLookup) * m)) != Q1_OK) return st;
+    if ((st = L->h_lookup.alloc(sizeof(CubeLookup) * m)) != Q1_OK) return st;
+    if ((st = L->d_status.alloc(16)) != Q1_OK) return st;
+    if ((st = L->h_status.alloc(16)) != Q1_OK) return st;
+    Q1_CUDA(cudaMemset(L->d_status.p, 0, 16));
+    *L->h_status.as<uint32_t>() = 0;
+    return grow_items(L, 4096);
 }
 
 // Makes the request's table resident (or finds it) and pins it; false if it cannot be placed
@@ -388,6 +453,7 @@ bool admit_table(q1_server* s, Ticket* t) {
                 victim = c;
         if (victim == s->cache.end()) return false;
         s->arena.release(victim->second.off, victim->second.len);
+        if (victim->second.gen_ev) cudaEventDestroy(victim->second.gen_ev);   // released once it completes
         s->cache.erase(victim);
         s->evictions++;
     }
@@ -411,9 +477,15 @@ TablePtrs table_ptrs(q1_server* s, const Ticket* t) {
     return TablePtrs{s->arena_mem.as<uint8_t>(t->table->off), TableLayout(t->req.adhoc_rows)};
 }
 
-// Generates the ticket's table if it is not resident yet (stream order puts it before readers).
+// Generates the ticket's table on the lane's stream if it is not resident yet; a table that another
+// lane generated is waited for through its event (a no-op once that generation has finished).
 q1_status ensure_generated(q1_server* s, Ticket* t, cudaStream_t st) {
-    if (t->table->ready) return Q1_OK;
+    std::lock_guard<std::mutex> lk(s->m);
+    CachedTable* tab = t->table;
+    if (tab->ready) {
+        if (tab->gen_ev && tab->gen_stream != st) Q1_CUDA(cudaStreamWaitEvent(st, tab->gen_ev, 0));
+        return Q1_OK;
+    }
     const TablePtrs tp = table_ptrs(s, t);
     uint8_t* tb = tp.base;
     const TableLayout& L = tp.L;
@@ -421,23 +493,28 @@ q1_status ensure_generated(q1_server* s, Ticket* t, cudaStream_t st) {
                     tb + L.off[3], tb + L.off[1], reinterpret_cast<uint32_t*>(tb + L.off[5])};
     const bool flags = t->req.grouping == Q1_GROUP_FLAGS;
     Q1_CUDA(launch_generate_keyed_table(t->req.adhoc_seed, t->req.adhoc_rows, flags ? 1u : 0u, groups_of(t->req), o, st));
-    t->table->ready = true;
+    if (!tab->gen_ev) Q1_CUDA(cudaEventCreateWithFlags(&tab->gen_ev, cudaEventDisableTiming));
+    Q1_CUDA(cudaEventRecord(tab->gen_ev, st));
+    tab->gen_stream = st;
+    tab->ready = true;
     s->generated_rows += t->req.adhoc_rows;
     return Q1_OK;
 }
 
-// Enqueues one batched round for the admitted tickets on the server stream.
-q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
+// Enqueues one batched round for the lane's tickets on the lane's streams.
+q1_status enqueue_round(q1_server* s, Lane* Ln) {
+    const std::vector<Ticket*>& batch = Ln->batch;
     const uint32_t n = (uint32_t)batch.size();
-    cudaStream_t st = s->stream;
-    BatchInstanceDev* inst = s->h_inst.as<BatchInstanceDev>();
-    uint64_t* base = s->h_base.as<uint64_t>();
-    CubeLookup* look = s->h_lookup.as<CubeLookup>();
+    cudaStream_t st = Ln->stream;
+    BatchInstanceDev* inst = Ln->h_inst.as<BatchInstanceDev>();
+    uint64_t* base = Ln->h_base.as<uint64_t>();
+    CubeLookup* look = Ln->h_lookup.as<CubeLookup>();
     uint32_t ninst = 0, nlook = 0;
     uint64_t groups = 0, tiles = 0;
     base[0] = 0;
     q1_status r;
-    Q1_CUDA(cudaMemsetAsync(s->d_resp.p, 0, (uint64_t)n * kRespWords * 8, st));
+    Q1_CUDA(cudaMemsetAsync(Ln->d_status.p, 0, 4, st));
+    Q1_CUDA(cudaMemsetAsync(Ln->d_resp.p, 0, (uint64_t)n * kRespWords * 8, st));
     for (uint32_t i = 0; i < n; ++i) {
         Ticket* t = batch[i];
         const bool flags = t->req.grouping == Q1_GROUP_FLAGS;
@@ -462,8 +539,8 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
         d.cutoff = cut;
         d.num_groups = kg;
         d.mode = kg <= 4 ? kModeRegisters : kModeShared;
-        d.acc = s->d_scratch.as<unsigned long long>() + 8 * groups;
-        d.out = s->d_resp.as<unsigned long long>() + (uint64_t)i * kRespWords;
+        d.acc = Ln->d_scratch.as<unsigned long long>() + 8 * groups;
+        d.out = Ln->d_resp.as<unsigned long long>() + (uint64_t)i * kRespWords;
         groups += kg;
         base[ninst + 1] = groups;
         tiles += (d.rows + kBatchTileRows - 1) / kBatchTileRows;
@@ -475,29 +552,30 @@ q1_status enqueue_round(q1_server* s, const std::vector<Ticket*>& batch) {
         std::vector<BatchItem> items;
         BatchParams prm{};
         batch_plan(inst, ninst, (uint32_t)chunk, (uint32_t)s->di->sm_count, items, prm);
-        if ((r = grow_items(s, items.size())) != Q1_OK) return r;
+        if ((r = grow_items(Ln, items.size())) != Q1_OK) return r;
         if (!items.empty()) {
-            memcpy(s->h_items.p, items.data(), sizeof(BatchItem) * items.size());
-            Q1_CUDA(cudaMemcpyAsync(s->d_items.p, s->h_items.p, sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
+            memcpy(Ln->h_items.p, items.data(), sizeof(BatchItem) * items.size());
+            Q1_CUDA(cudaMemcpyAsync(Ln->d_items.p, Ln->h_items.p, sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice, st));
         }
-        Q1_CUDA(cudaMemcpyAsync(s->d_inst.p, inst, sizeof(BatchInstanceDev) * ninst, cudaMemcpyHostToDevice, st));
-        Q1_CUDA(cudaMemcpyAsync(s->d_base.p, base, sizeof(uint64_t) * (ninst + 1), cudaMemcpyHostToDevice, st));
-        Q1_CUDA(cudaMemsetAsync(s->d_scratch.p, 0, groups * 64, st));
+        Q1_CUDA(cudaMemcpyAsync(Ln->d_inst.p, inst, sizeof(BatchInstanceDev) * ninst, cudaMemcpyHostToDevice, st));
+        Q1_CUDA(cudaMemcpyAsync(Ln->d_base.p, base, sizeof(uint64_t) * (ninst + 1), cudaMemcpyHostToDevice, st));
+        Q1_CUDA(cudaMemsetAsync(Ln->d_scratch.p, 0, groups * 64, st));
         if (!items.empty()) {
-            Q1_CUDA(cudaMemsetAsync(s->d_cursor.p, 0, 4 * kEngines, st));
-            prm.inst = s->d_inst.as<BatchInstanceDev>();
-            prm.items = s->d_items.as<BatchItem>();
-            prm.cursor = s->d_cursor.as<uint32_t>();
-            prm.status = s->di->status;
-            Q1_CUDA(launch_batch(prm, prm.grid_regs, prm.grid_tables, st, s->aux, s->fork, s->join));
+            Q1_CUDA(cudaMemsetAsync(Ln->d_cursor.p, 0, 4 * kEngines, st));
+            prm.inst = Ln->d_inst.as<BatchInstanceDev>();
+            prm.items = Ln->d_items.as<BatchItem>();
+            prm.cursor = Ln->d_cursor.as<uint32_t>();
+            prm.status = Ln->d_status.as<uint32_t>();
+            Q1_CUDA(launch_batch(prm, prm.grid_regs, prm.grid_tables, st, Ln->aux, Ln->fork, Ln->join));
         }
-        Q1_CUDA(launch_batch_finalize(s->d_inst.as<BatchInstanceDev>(), s->d_base.as<uint64_t>(), ninst, groups, st));
+        Q1_CUDA(launch_batch_finalize(Ln->d_inst.as<BatchInstanceDev>(), Ln->d_base.as<uint64_t>(), ninst, groups, st));
     }
     if (nlook) {
-        Q1_CUDA(cudaMemcpyAsync(s->d_lookup.p, look, sizeof(CubeLookup) * nlook, cudaMemcpyHostToDevice, st));
-        Q1_CUDA(launch_cube_lookup(s->d_lookup.as<CubeLookup>(), nlook, kRespWords, s->d_resp.as<unsigned long long>(), st));
+        Q1_CUDA(cudaMemcpyAsync(Ln->d_lookup.p, look, sizeof(CubeLookup) * nlook, cudaMemcpyHostToDevice, st));
+        Q1_CUDA(launch_cube_lookup(Ln->d_lookup.as<CubeLookup>(), nlook, kRespWords, Ln->d_resp.as<unsigned long long>(), st));
     }
-    Q1_CUDA(cudaMemcpyAsync(s->h_resp.p, s->d_resp.p, (uint64_t)n * kRespWords * 8, cudaMemcpyDeviceToHost, st));
+    Q1_CUDA(cudaMemcpyAsync(Ln->h_resp.p, Ln->d_resp.p, (uint64_t)n * kRespWords * 8, cudaMemcpyDeviceToHost, st));
+    Q1_CUDA(cudaMemcpyAsync(Ln->h_status.p, Ln->d_status.p, 4, cudaMemcpyDeviceToHost, st));
     return Q1_OK;
 }
 
@@ -513,10 +591,11 @@ q1_status plain_launch(const q1_request& req, const q1_compressed_columns& c, co
 }
 
 // Q1_SERVE_PLAIN: one request, one plain launch over the resident or cached table.
-q1_status enqueue_plain(q1_server* s, Ticket* t) {
-    cudaStream_t st = s->stream;
+q1_status enqueue_plain(q1_server* s, Lane* Ln) {
+    Ticket* t = Ln->batch[0];
+    cudaStream_t st = Ln->stream;
     t->groups = groups_of(t->req);
-    Q1_CUDA(cudaMemsetAsync(s->d_resp.p, 0, kRespWords * 8, st));
+    Q1_CUDA(cudaMemsetAsync(Ln->d_resp.p, 0, kRespWords * 8, st));
     q1_compressed_columns c{};
     const uint32_t* keys = nullptr;
     uint64_t rows = 0;
@@ -536,20 +615,43 @@ q1_status enqueue_plain(q1_server* s, Ticket* t) {
         rows = t->req.adhoc_rows;
     }
     const uint32_t G = t->req.kind == Q1_REQ_RESIDENT ? t->groups : key_groups(t->req);
-    if ((r = plain_launch(t->req, c, keys, G, rows, s->plain_scratch.p, s->d_resp.as<q1_i128>(), st)) != Q1_OK) return r;
-    Q1_CUDA(cudaMemcpyAsync(s->h_resp.p, s->d_resp.p, (uint64_t)G * 12 * 8, cudaMemcpyDeviceToHost, st));
+    if ((r = plain_launch(t->req, c, keys, G, rows, s->plain_scratch.p, Ln->d_resp.as<q1_i128>(), st)) != Q1_OK) return r;
+    Q1_CUDA(cudaMemcpyAsync(Ln->h_resp.p, Ln->d_resp.p, (uint64_t)G * 12 * 8, cudaMemcpyDeviceToHost, st));
     return Q1_OK;
 }
 
-void run_round(q1_server* s, const std::vector<Ticket*>& batch) {
-    q1_status r = s->opts.mode == Q1_SERVE_PLAIN ? enqueue_plain(s, batch[0]) : enqueue_round(s, batch);
-    // drain the stream even after a failed enqueue, before any buffer is reused
-    const q1_status r2 = check_device_status(s->stream, s->di->status);
-    if (r == Q1_OK) r = r2;
-    const std::string err = r == Q1_OK ? std::string() : std::string(q1_last_error());
+// Completer thread: waits for the lane's round, then answers its tickets. Rounds retire in the
+// order they were enqueued; a round behind a failed one fails too (the device state is suspect).
+void retire_round(q1_server* s, Lane* Ln) {
+    const std::vector<Ticket*>& batch = Ln->batch;
+    q1_status r = Ln->enq;
+    std::string err = Ln->err;
+    // drain the lane even after a failed enqueue, before any of its buffers is reused
+    const cudaError_t se = cudaStreamSynchronize(Ln->stream);
+    const cudaError_t sa = cudaStreamSynchronize(Ln->aux);
+    if (r == Q1_OK && (se != cudaSuccess || sa != cudaSuccess)) {
+        r = cuda_error(se != cudaSuccess ? se : sa, "serving round");
+        err = q1_last_error();
+    }
+    if (r == Q1_OK) {
+        if (s->opts.mode == Q1_SERVE_PLAIN) {
+            // the plain launch reports through the device's status word (one lane in this mode)
+            r = check_device_status(Ln->stream, s->di->status);
+        } else {
+            const uint32_t bits = *Ln->h_status.as<volatile uint32_t>();
+            if (bits & 1u) r = set_error(Q1_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+            else if (bits & 4u) r = set_error(Q1_ERR_INTERNAL, "a device work buffer would have overflowed");
+            else if (bits) r = set_error(Q1_ERR_DOMAIN, "a row is outside the kernels' domain");
+        }
+        if (r != Q1_OK) err = q1_last_error();
+    }
     const double when = now_ms();
-    const unsigned long long* words = s->h_resp.as<unsigned long long>();
+    const unsigned long long* words = Ln->h_resp.as<unsigned long long>();
     std::lock_guard<std::mutex> lk(s->m);
+    if (r == Q1_OK && s->fatal != Q1_OK) {
+        r = s->fatal;
+        err = s->fatal_msg;
+    }
     for (size_t i = 0; i < batch.size(); ++i) {
         Ticket* t = batch[i];
         if (r == Q1_OK) {
@@ -581,18 +683,36 @@ void run_round(q1_server* s, const std::vector<Ticket*>& batch) {
         s->fatal = r;
         s->fatal_msg = err;
     }
+    Ln->batch.clear();
+    s->inflight.pop_front();
+    s->free_lanes.push_back(Ln);
+    s->cv_work.notify_all();
     s->cv_done.notify_all();
+}
+
+void completer_loop(q1_server* s) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        Lane* Ln;
+        {
+            std::unique_lock<std::mutex> lk(s->m);
+            s->cv_retire.wait(lk, [&] { return !s->inflight.empty() || s->dispatcher_done; });
+            if (s->inflight.empty()) return;   // the dispatcher has stopped and every round retired
+            Ln = s->inflight.front();
+        }
+        retire_round(s, Ln);
+    }
 }
 
 void dispatcher_loop(q1_server* s) {
     cudaSetDevice(s->device);
     const uint32_t slots = s->opts.mode == Q1_SERVE_PLAIN ? 1u : s->opts.max_inflight;
     for (;;) {
-        std::vector<Ticket*> batch;
+        Lane* Ln = nullptr;
         {
             std::unique_lock<std::mutex> lk(s->m);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
-            if (s->pending.empty()) return;   // stop requested and the queue is drained
+            s->cv_work.wait(lk, [&] { return (s->stop && s->pending.empty()) || (!s->pending.empty() && !s->free_lanes.empty()); });
+            if (s->pending.empty()) break;   // stop requested and the queue is drained
             if (s->fatal != Q1_OK) {
                 // after a failed round the device state is suspect: fail what is queued
                 const double when = now_ms();
@@ -601,20 +721,42 @@ void dispatcher_loop(q1_server* s) {
                 s->cv_done.notify_all();
                 continue;
             }
+            Ln = s->free_lanes.front();
             // admit from the head while a slot is free and the next table is or can be resident
-            while (!s->pending.empty() && batch.size() < slots) {
+            while (!s->pending.empty() && Ln->batch.size() < slots) {
                 Ticket* t = s->pending.front();
                 if (t->req.kind == Q1_REQ_ADHOC && !admit_table(s, t)) break;   // with a later round
                 t->t_admit = now_ms();
-                batch.push_back(t);
+                Ln->batch.push_back(t);
                 s->pending.pop_front();
             }
-            s->admitted_total += batch.size();
+            if (Ln->batch.empty()) {
+                // The head's table cannot be placed while running rounds pin the arena; with no
+                // round running nothing is pinned and any table that submission accepted fits.
+                if (s->inflight.empty()) {
+                    Ticket* t = s->pending.front();
+                    s->pending.pop_front();
+                    complete(s, t, set_error(Q1_ERR_BUSY, "ad-hoc table does not fit the arena"), now_ms());
+                    s->cv_done.notify_all();
+                } else {
+                    s->cv_work.wait(lk);   // until a round retires and unpins its tables
+                }
+                continue;
+            }
+            s->free_lanes.pop_front();
+            s->admitted_total += Ln->batch.size();
+            if (!s->inflight.empty()) s->overlapped_rounds++;
+            s->max_in_flight = std::max<uint32_t>(s->max_in_flight, (uint32_t)s->inflight.size() + 1);
         }
-        // Rounds run one at a time, so no table is pinned when a round starts forming and every
-        // table that submission accepted fits after evictions: a round is never empty.
-        if (!batch.empty()) run_round(s, batch);
+        Ln->enq = s->opts.mode == Q1_SERVE_PLAIN ? enqueue_plain(s, Ln) : enqueue_round(s, Ln);
+        Ln->err = Ln->enq == Q1_OK ? std::string() : std::string(q1_last_error());
+        std::lock_guard<std::mutex> lk(s->m);
+        s->inflight.push_back(Ln);
+        s->cv_retire.notify_one();
     }
+    std::lock_guard<std::mutex> lk(s->m);
+    s->dispatcher_done = true;
+    s->cv_retire.notify_one();
 }
 
 }  // namespace
@@ -626,6 +768,7 @@ void q1_server_opts_default(q1_server_opts* o) {
     memset(o, 0, sizeof(*o));
     o->device = 0;
     o->max_inflight = 256;
+    o->max_rounds_in_flight = 2;
     o->seed = 20260104;
     o->resident_rows = 600000000ull;
     o->hbm_budget_bytes = 120ull << 30;
@@ -640,6 +783,9 @@ q1_status q1_server_open(const q1_server_opts* opts, q1_server** out) {
     if (opts) s->opts = *opts;
     if (s->opts.max_inflight < 1 || s->opts.max_inflight > 65536)
         return set_error(Q1_ERR_INVALID_ARGUMENT, "max_inflight must be in 1..65536");
+    if (s->opts.max_rounds_in_flight == 0) s->opts.max_rounds_in_flight = 2;
+    if (s->opts.max_rounds_in_flight > 8)
+        return set_error(Q1_ERR_INVALID_ARGUMENT, "max_rounds_in_flight must be in 0..8 (0 = 2)");
     if (s->opts.resident_rows > (1ull << 40)) return set_error(Q1_ERR_INVALID_ARGUMENT, "resident table too large");
     if (s->opts.max_adhoc_rows > (uint64_t)UINT32_MAX * kBatchTileRows)
         return set_error(Q1_ERR_INVALID_ARGUMENT, "max_adhoc_rows too large");
@@ -649,27 +795,19 @@ q1_status q1_server_open(const q1_server_opts* opts, q1_server** out) {
     if (st != Q1_OK) return st;
     Q1_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     Q1_CUDA(cudaStreamCreateWithFlags(&s->plain_stream, cudaStreamNonBlocking));
-    Q1_CUDA(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
-    Q1_CUDA(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
-    Q1_CUDA(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
     Q1_CUDA(batch_prepare_launch());
     s->res_rows = s->opts.resident_rows;
     if ((st = build_resident(s.get())) != Q1_OK) return st;
     if ((st = s->arena_mem.alloc(s->opts.hbm_budget_bytes)) != Q1_OK) return st;
     s->arena.reset(s->opts.hbm_budget_bytes);
-    const uint64_t m = s->opts.max_inflight;
-    if ((st = s->d_resp.alloc(m * kRespWords * 8)) != Q1_OK) return st;
-    if ((st = s->h_resp.alloc(m * kRespWords * 8)) != Q1_OK) return st;
-    if ((st = s->d_inst.alloc(sizeof(BatchInstanceDev) * m)) != Q1_OK) return st;
-    if ((st = s->h_inst.alloc(sizeof(BatchInstanceDev) * m)) != Q1_OK) return st;
-    if ((st = s->d_base.alloc(sizeof(uint64_t) * (m + 1))) != Q1_OK) return st;
-    if ((st = s->h_base.alloc(sizeof(uint64_t) * (m + 1))) != Q1_OK) return st;
-    if ((st = s->d_scratch.alloc(m * kMaxGroups * 64)) != Q1_OK) return st;
-    if ((st = s->d_cursor.alloc(4 * kEngines)) != Q1_OK) return st;
-    if ((st = s->d_lookup.alloc(sizeof(CubeLookup) * m)) != Q1_OK) return st;
-    if ((st = s->h_lookup.alloc(sizeof(CubeLookup) * m)) != Q1_OK) return st;
-    if ((st = grow_items(s.get(), 4096)) != Q1_OK) return st;
+    const uint32_t nlanes = s->opts.mode == Q1_SERVE_PLAIN ? 1u : s->opts.max_rounds_in_flight;
+    for (uint32_t i = 0; i < nlanes; ++i) {
+        s->lanes.emplace_back(new Lane());
+        if ((st = lane_open(s->lanes.back().get(), s->opts.max_inflight)) != Q1_OK) return st;
+        s->free_lanes.push_back(s->lanes.back().get());
+    }
     if ((st = s->plain_scratch.alloc(q1_groupkey_scratch_bytes(kMaxGroups))) != Q1_OK) return st;
+    s->completer = std::thread(completer_loop, s.get());
     s->dispatcher = std::thread(dispatcher_loop, s.get());
     *out = s.release();
     return Q1_OK;
@@ -737,6 +875,8 @@ q1_status q1_server_stats_get(q1_server* s, q1_server_stats* out) {
     for (const auto& e : s->cache) out->cached_bytes += e.second.len;
     out->wall_ms = s->t_last > s->t_first ? s->t_last - s->t_first : 0;
     out->mean_round_size = s->rounds ? (double)s->admitted_total / (double)s->rounds : 0;
+    out->overlapped_rounds = s->overlapped_rounds;
+    out->max_rounds_in_flight = s->max_in_flight;
     std::vector<double> l = s->latencies;
     if (!l.empty()) {
         std::sort(l.begin(), l.end());
@@ -760,6 +900,8 @@ q1_status q1_server_reset_stats(q1_server* s) {
     s->latencies.clear();
     s->rounds = s->completed = s->failed = s->logical_rows = s->scanned_rows = s->admitted_total = 0;
     s->generated_rows = s->cache_hits = s->cache_misses = s->evictions = 0;
+    s->overlapped_rounds = 0;
+    s->max_in_flight = 0;
     s->t_first = s->t_last = 0;
     return Q1_OK;
 }
@@ -855,7 +997,16 @@ q1_status q1_server_close(q1_server* s) {
     }
     s->cv_work.notify_all();
     if (s->dispatcher.joinable()) s->dispatcher.join();
+    else {
+        std::lock_guard<std::mutex> lk(s->m);   // open failed before the dispatcher started
+        s->dispatcher_done = true;
+    }
+    s->cv_retire.notify_all();
+    if (s->completer.joinable()) s->completer.join();
     cudaSetDevice(s->device);
+    s->lanes.clear();
+    for (auto& e : s->cache)
+        if (e.second.gen_ev) cudaEventDestroy(e.second.gen_ev);
     if (s->stream) {
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
@@ -864,9 +1015,6 @@ q1_status q1_server_close(q1_server* s) {
         cudaStreamSynchronize(s->plain_stream);
         cudaStreamDestroy(s->plain_stream);
     }
-    if (s->aux) cudaStreamDestroy(s->aux);
-    if (s->fork) cudaEventDestroy(s->fork);
-    if (s->join) cudaEventDestroy(s->join);
     delete s;
     return Q1_OK;
 }
