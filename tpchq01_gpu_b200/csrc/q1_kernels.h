@@ -37,6 +37,12 @@ inline constexpr uint32_t kStages = (P == kPlaceSharedMemPerThread) ? 3u : 4u;
 #define Q1_CONSUMER_WARPS 8
 #endif
 inline constexpr uint32_t kConsumerWarps = Q1_CONSUMER_WARPS;
+// Tiles a warp of the global placement write-combines in registers between its atomic adds into
+// the global table (each warp adds 16 rows per thread of a 4096-row tile).
+#ifndef Q1_GLOBAL_FLUSH_TILES
+#define Q1_GLOBAL_FLUSH_TILES 16
+#endif
+inline constexpr uint32_t kGlobalFlushTiles = Q1_GLOBAL_FLUSH_TILES;
 
 struct ScanParams {
     const uint8_t* col[7];      // column base pointers in tile order; 16-byte aligned

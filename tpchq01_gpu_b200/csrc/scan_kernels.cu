@@ -291,6 +291,8 @@ struct AccPerThread {
     __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    template <class P>
+    __device__ __forceinline__ void finish(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
         fold();
 #pragma unroll
@@ -340,6 +342,8 @@ struct AccWarpLane {
     __device__ __forceinline__ bool owns(uint32_t c) const { return c == my; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    template <class P>
+    __device__ __forceinline__ void finish(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
         fold();
         if (lane < (32u / G) * G) {
@@ -350,25 +354,32 @@ struct AccWarpLane {
 };
 
 // --- local_mem (src/kernels/ht_in_local_mem.cuh:11-74): per-thread tables indexed by the row's
-// group, which places them in (L1-cached) local memory.
+// group, which places them in (L1-cached) local memory. A group's entry is four 64-bit words
+// (five for reference-typed columns, whose quantity needs a word of its own): the count, quantity
+// and discount share one word, since a thread adds at most 2^15 rows per launch
+// (count < 2^16, quantity <= 255 * 2^15 < 2^23, discount <= 100 * 2^15 < 2^22), then price,
+// (100 - d) price and (100 - d)(100 + t) price. A row is one read-modify-write per word.
 template <int G, bool kWideQty>
 struct AccLocal {
-    uint64_t t[G][5];   // p, dp, ch, q, d
-    uint32_t cnt[G];
+    static constexpr int kWords = kWideQty ? 5 : 4;
+    static constexpr int kQtyShift = 16, kDiscShift = kWideQty ? 16 : 39;
+    uint64_t t[G][kWords];   // [0] count | quantity << 16 | discount << 39 (or count | discount << 16), [1] p,
+                             // [2] (100-d) p, [3] (100-d)(100+t) p, [4] quantity (reference-typed columns)
     __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
-        for (int i = 0; i < G; ++i) {
-            for (int j = 0; j < 5; ++j) t[i][j] = 0;
-            cnt[i] = 0;
-        }
+        for (int i = 0; i < G; ++i)
+            for (int j = 0; j < kWords; ++j) t[i][j] = 0;
     }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
         if (c < (uint32_t)G) {
-            t[c][0] += p;
-            t[c][1] = mad_wide(a, p, t[c][1]);
-            t[c][2] = mad_wide(ab, p, t[c][2]);
-            t[c][3] += q;
-            t[c][4] += d;
-            cnt[c] += 1;
+            if constexpr (kWideQty) {
+                t[c][0] += 1ull | ((uint64_t)d << kDiscShift);
+                t[c][4] += q;
+            } else {
+                t[c][0] += 1ull | ((uint64_t)q << kQtyShift) | ((uint64_t)d << kDiscShift);
+            }
+            t[c][1] += p;
+            t[c][2] = mad_wide(a, p, t[c][2]);
+            t[c][3] = mad_wide(ab, p, t[c][3]);
         }
     }
     __device__ __forceinline__ void add_quad(const Quad& x) {
@@ -377,14 +388,17 @@ struct AccLocal {
             add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
     }
     __device__ __forceinline__ void fold() {}
-    // whether this thread sums the rows of group code c (every thread reads every row it is given)
     __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    template <class P>
+    __device__ __forceinline__ void finish(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
 #pragma unroll
         for (int i = 0; i < G; ++i) {
-            const uint64_t vals[kNumAggs] = {cnt[i], t[i][3], t[i][0], t[i][4], t[i][1], t[i][2]};
+            const uint64_t w0 = t[i][0];
+            const uint64_t qty = kWideQty ? t[i][kWords - 1] : (w0 >> kQtyShift) & ((1ull << 23) - 1);
+            const uint64_t vals[kNumAggs] = {w0 & 0xFFFFull, qty, t[i][1], w0 >> kDiscShift, t[i][2], t[i][3]};
 #pragma unroll
             for (int a = 0; a < kNumAggs; ++a) {
                 uint64_t lo = vals[a], hi = 0;
@@ -433,6 +447,8 @@ struct AccSharedPerThread {
     __device__ __forceinline__ bool owns(uint32_t) const { return true; }
     template <class P>
     __device__ __forceinline__ void tile_done(const P&, uint32_t) {}
+    template <class P>
+    __device__ __forceinline__ void finish(const P&, uint32_t) {}
     __device__ __forceinline__ void flush(CtaRed red, uint32_t lane) {
         const uint32_t stride = G * nthreads;
 #pragma unroll
@@ -451,22 +467,42 @@ struct AccSharedPerThread {
 };
 
 // --- global (src/kernels/ht_in_global_mem.hpp:11-52): no thread- or block-private table; the
-// aggregates live only in the global output. The reference issues 6 atomics per row; here each
-// warp first combines its rows of one tile (a register buffer emptied after every tile) and then
-// issues one 64-bit atomic per (group, aggregate) straight into the global table.
+// aggregates live only in the global output, updated by atomics all through the scan. The
+// reference issues 6 atomics per row; here each warp write-combines its rows of
+// kGlobalFlushTiles tiles in a register buffer, then issues one 128-bit atomic add per
+// (group, aggregate) straight into the global table and empties the buffer.
 template <int G, bool kWideQty>
 struct AccGlobal {
+    // A warp's flush of one sum is a 64-bit warp reduction: at most 32 lanes x 16 rows x 128
+    // tiles of charges below 100 (2^32 - 1) 355 < 2^47.2 stays below 2^64.
+    static_assert(kGlobalFlushTiles >= 1 && kGlobalFlushTiles <= 128, "flush sums must stay below 2^64");
     AccPerThread<G, kWideQty> buf;
-    __device__ __forceinline__ void init(uint32_t a, uint32_t b, uint8_t* s) { buf.init(a, b, s); }
+    uint32_t tiles;
+    __device__ __forceinline__ void init(uint32_t a, uint32_t b, uint8_t* s) {
+        buf.init(a, b, s);
+        tiles = 0;
+    }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
         buf.add(c, q, d, a, ab, p);
     }
     __device__ __forceinline__ void add_quad(const Quad& x) { buf.add_quad(x); }
     __device__ __forceinline__ void fold() { buf.fold(); }
     __device__ __forceinline__ bool owns(uint32_t) const { return true; }
+    // Called by all lanes after each tile (warp-uniform count).
     template <class P>
     __device__ __forceinline__ void tile_done(const P& prm, uint32_t lane) {
         buf.fold();
+        if (++tiles < kGlobalFlushTiles) return;
+        to_global(prm, lane);
+    }
+    template <class P>
+    __device__ __forceinline__ void finish(const P& prm, uint32_t lane) {
+        buf.fold();
+        if (tiles) to_global(prm, lane);
+    }
+    template <class P>
+    __device__ __forceinline__ void to_global(const P& prm, uint32_t lane) {
+        tiles = 0;
 #pragma unroll
         for (int i = 0; i < G; ++i) {
             const int grp = G == 4 ? prm.pair_group[i] : i;
@@ -768,6 +804,7 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
             }
             acc.tile_done(prm, lane);
         }
+        acc.finish(prm, lane);
         if (bad && prm.status) atomicOr(prm.status, kStatusDomain);
         acc.flush(CtaRed{red}, lane);
     }
