@@ -1094,6 +1094,36 @@ def serve_trace(rate, duration, pool, seed):
     return arrivals, reqs
 
 
+def percentile(values, pct):
+    if not values:
+        return None
+    v = sorted(values)
+    return v[min(len(v) - 1, int(round(pct / 100.0 * (len(v) - 1))))]
+
+
+def closed_loop(L, _lib, h, reqs):
+    """Capacity: every request submitted at once, then all waited for."""
+    import ctypes
+    if not reqs:
+        return {"requests": 0}
+    _lib.check(L.q1_server_reset_stats(h))
+    t0 = time.perf_counter()
+    tks = []
+    for r in reqs:
+        t = ctypes.c_uint64()
+        _lib.check(L.q1_server_submit(h, ctypes.byref(_lib.Request(*r)), ctypes.byref(t)))
+        tks.append(t.value)
+    for t in tks:
+        _lib.check(L.q1_server_wait(h, t, 600_000, ctypes.byref(_lib.Response())))
+    cap_s = time.perf_counter() - t0
+    cst = _lib.ServerStats()
+    _lib.check(L.q1_server_stats_get(h, ctypes.byref(cst)))
+    return {"requests": len(reqs), "wall_s": cap_s, "requests_per_s": len(reqs) / cap_s,
+            "logical_rows_per_s": cst.logical_rows / cap_s, "scanned_rows_per_s": cst.scanned_rows / cap_s,
+            "rounds": cst.rounds, "mean_round_size": cst.mean_round_size, "p50_ms": cst.p50_ms, "p99_ms": cst.p99_ms,
+            "overlapped_rounds": cst.overlapped_rounds}
+
+
 def run_trace(q, _lib, h, arrivals, reqs, limit_s):
     """Submits at the trace's times (open loop) from this thread, waits from another."""
     import ctypes
@@ -1198,24 +1228,22 @@ def run_serve(args):
                 b_ = bytes(resp_j.aggregates)[: g * 96]
                 same = same and a == b_ and results[i][0] == 0
             wall = st.wall_ms / 1e3
-            # capacity: the first requests of the trace submitted at once (closed loop)
-            cap_n = min(len(reqs), 5000)
-            _lib.check(L.q1_server_reset_stats(h))
-            t0 = time.perf_counter()
-            tks = []
-            for r in reqs[:cap_n]:
-                t = ctypes.c_uint64()
-                _lib.check(L.q1_server_submit(h, ctypes.byref(_lib.Request(*r)), ctypes.byref(t)))
-                tks.append(t.value)
-            for t in tks:
-                _lib.check(L.q1_server_wait(h, t, 600_000, ctypes.byref(_lib.Response())))
-            cap_s = time.perf_counter() - t0
-            cst = _lib.ServerStats()
-            _lib.check(L.q1_server_stats_get(h, ctypes.byref(cst)))
-            capacity = {"requests": cap_n, "wall_s": cap_s, "requests_per_s": cap_n / cap_s,
-                        "logical_rows_per_s": cst.logical_rows / cap_s, "scanned_rows_per_s": cst.scanned_rows / cap_s,
-                        "rounds": cst.rounds, "mean_round_size": cst.mean_round_size}
-            out[mode_name] = {"capacity": capacity, "submitted": submitted, "completed": st.completed, "ok": ok, "failed": st.failed,
+            # latency and rows/s at the offered rate, per request kind
+            per_kind = {}
+            for kind, kname in [(0, "resident"), (1, "adhoc")]:
+                lat = [results[i][1].latency_ms for i in results if reqs[i][0] == kind and results[i][0] == 0]
+                rows_k = sum(ROWS if kind == 0 else reqs[i][4] for i in results
+                             if reqs[i][0] == kind and results[i][0] == 0)
+                per_kind[kname] = {"completed": len(lat), "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
+                                   "logical_rows_per_s": rows_k / wall if wall else None}
+            # capacity: the first requests of the trace submitted at once (closed loop), the mix and
+            # each kind alone
+            capacity = closed_loop(L, _lib, h, reqs[: min(len(reqs), 5000)])
+            capacity_kind = {kname: closed_loop(L, _lib, h, [r for r in reqs if r[0] == kind][:2000])
+                             for kind, kname in [(0, "resident"), (1, "adhoc")]}
+            out[mode_name] = {"capacity": capacity, "capacity_by_kind": capacity_kind, "by_kind": per_kind,
+                              "overlapped_rounds": st.overlapped_rounds, "max_rounds_in_flight": st.max_rounds_in_flight,
+                              "submitted": submitted, "completed": st.completed, "ok": ok, "failed": st.failed,
                               "rounds": st.rounds, "mean_round_size": st.mean_round_size,
                               "p50_ms": st.p50_ms, "p90_ms": st.p90_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
                               "mean_ms": st.mean_ms, "wall_s": wall,
@@ -1228,6 +1256,9 @@ def run_serve(args):
         finally:
             L.q1_server_close(h)
     s_, p_ = out["served"], out["plain"]
+    out["speedup_capacity_by_kind"] = {
+        k: s_["capacity_by_kind"][k]["logical_rows_per_s"] / p_["capacity_by_kind"][k]["logical_rows_per_s"]
+        for k in ["resident", "adhoc"] if p_["capacity_by_kind"][k]["logical_rows_per_s"]}
     out["value"] = s_["capacity"]["logical_rows_per_s"]
     out["speedup_capacity_rows_per_s"] = s_["capacity"]["logical_rows_per_s"] / p_["capacity"]["logical_rows_per_s"]
     out["speedup_at_offered_rate_rows_per_s"] = (s_["logical_rows_per_s"] or 0) / max(p_["logical_rows_per_s"] or 1e-9,
