@@ -23,36 +23,49 @@ namespace q1 {
 // Host memory read rate (q1_measure_host_read)
 // ---------------------------------------------------------------------------------------------
 
-// XOR of every 16-byte word of [p, p + bytes) (bytes a multiple of 16, p 16-byte aligned), four
-// independent accumulators so that loads, not the reduction, set the pace.
-static __m128i xor_words(const __m128i* p, uint64_t words) {
-    __m128i a = _mm_setzero_si128(), b = a, c = a, d = a;
+// XOR of every 64-byte line of [p, p + 64 * lines) (p 64-byte aligned), eight independent
+// accumulators so that loads, not the reduction, set the pace; AVX-512 where the host has it.
+__attribute__((target("avx512f"))) static uint64_t xor_lines_avx512(const uint8_t* p, uint64_t lines) {
+    __m512i a[8];
+    for (int k = 0; k < 8; ++k) a[k] = _mm512_setzero_si512();
     uint64_t i = 0;
-    for (; i + 4 <= words; i += 4) {
-        a = _mm_xor_si128(a, _mm_load_si128(p + i));
-        b = _mm_xor_si128(b, _mm_load_si128(p + i + 1));
-        c = _mm_xor_si128(c, _mm_load_si128(p + i + 2));
-        d = _mm_xor_si128(d, _mm_load_si128(p + i + 3));
+    for (; i + 8 <= lines; i += 8)
+        for (int k = 0; k < 8; ++k) a[k] = _mm512_xor_si512(a[k], _mm512_load_si512(p + 64 * (i + k)));
+    for (; i < lines; ++i) a[0] = _mm512_xor_si512(a[0], _mm512_load_si512(p + 64 * i));
+    for (int k = 1; k < 8; ++k) a[0] = _mm512_xor_si512(a[0], a[k]);
+    return (uint64_t)_mm512_reduce_or_epi64(a[0]);
+}
+
+__attribute__((target("avx2"))) static uint64_t xor_lines_avx2(const uint8_t* p, uint64_t lines) {
+    __m256i a[8];
+    for (int k = 0; k < 8; ++k) a[k] = _mm256_setzero_si256();
+    uint64_t i = 0;
+    for (; i + 4 <= lines; i += 4)
+        for (int k = 0; k < 8; ++k)
+            a[k] = _mm256_xor_si256(a[k], _mm256_load_si256(reinterpret_cast<const __m256i*>(p + 64 * i + 32 * k)));
+    for (; i < lines; ++i) {
+        a[0] = _mm256_xor_si256(a[0], _mm256_load_si256(reinterpret_cast<const __m256i*>(p + 64 * i)));
+        a[1] = _mm256_xor_si256(a[1], _mm256_load_si256(reinterpret_cast<const __m256i*>(p + 64 * i + 32)));
     }
-    for (; i < words; ++i) a = _mm_xor_si128(a, _mm_load_si128(p + i));
-    return _mm_xor_si128(_mm_xor_si128(a, b), _mm_xor_si128(c, d));
+    for (int k = 1; k < 8; ++k) a[0] = _mm256_xor_si256(a[0], a[k]);
+    return (uint64_t)_mm256_extract_epi64(a[0], 0) ^ (uint64_t)_mm256_extract_epi64(a[0], 3);
 }
 
 double host_read_gbs(const void* buf, uint64_t bytes, int threads) {
-    const uint64_t skip = (16 - (reinterpret_cast<uintptr_t>(buf) & 15)) & 15;
-    if (bytes <= skip + 16) return 0.0;
-    const __m128i* base = reinterpret_cast<const __m128i*>(static_cast<const uint8_t*>(buf) + skip);
-    const uint64_t words = (bytes - skip) / 16;
+    static const bool avx512 = __builtin_cpu_supports("avx512f");
+    const uint64_t skip = (64 - (reinterpret_cast<uintptr_t>(buf) & 63)) & 63;
+    if (bytes <= skip + 64) return 0.0;
+    const uint8_t* base = static_cast<const uint8_t*>(buf) + skip;
+    const uint64_t lines = (bytes - skip) / 64;
     if (threads < 1) threads = 1;
     std::vector<std::thread> ts;
     std::vector<uint64_t> out((size_t)threads);
-    const uint64_t per = (words + (uint64_t)threads - 1) / (uint64_t)threads;
+    const uint64_t per = (lines + (uint64_t)threads - 1) / (uint64_t)threads;
     const auto t0 = std::chrono::steady_clock::now();
     for (int t = 0; t < threads; ++t) {
-        const uint64_t b = std::min<uint64_t>(words, (uint64_t)t * per), e = std::min<uint64_t>(words, b + per);
+        const uint64_t b = std::min<uint64_t>(lines, (uint64_t)t * per), e = std::min<uint64_t>(lines, b + per);
         ts.emplace_back([&out, base, b, e, t] {
-            const __m128i x = xor_words(base + b, e - b);
-            out[(size_t)t] = (uint64_t)_mm_cvtsi128_si64(x) ^ (uint64_t)_mm_cvtsi128_si64(_mm_unpackhi_epi64(x, x));
+            out[(size_t)t] = avx512 ? xor_lines_avx512(base + 64 * b, e - b) : xor_lines_avx2(base + 64 * b, e - b);
         });
     }
     for (auto& t : ts) t.join();
@@ -60,7 +73,7 @@ double host_read_gbs(const void* buf, uint64_t bytes, int threads) {
     volatile uint64_t sink = 0;
     for (const uint64_t v : out) sink = sink ^ v;
     (void)sink;
-    return s > 0 ? (double)(words * 16) / s / 1e9 : 0.0;
+    return s > 0 ? (double)(lines * 64) / s / 1e9 : 0.0;
 }
 
 // ---------------------------------------------------------------------------------------------

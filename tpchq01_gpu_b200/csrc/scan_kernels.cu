@@ -353,12 +353,35 @@ struct AccWarpLane {
     }
 };
 
+// Sums of the rows of one group in a quad (W1: byte r is 1 iff row r is in the group): the packed
+// word count | quantity << 16 | discount << 39 (a thread adds at most 2^15 rows per launch, so
+// count < 2^16, quantity <= 255 * 2^15 < 2^23, discount <= 100 * 2^15 < 2^22) and price,
+// (100 - d) price and (100 - d)(100 + t) price.
+struct QuadGroupSums {
+    uint64_t w0, p, dp, ch;
+};
+__device__ __forceinline__ QuadGroupSums quad_group_sums(uint32_t W1, const Quad& x) {
+    QuadGroupSums s{0, 0, 0, 0};
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const uint32_t pg = __byte_perm(W1, 0u, 0x4440u | (uint32_t)r) * x.p[r];
+        s.p += pg;
+        s.dp = mad_wide(x.a[r], pg, s.dp);
+        s.ch = mad_wide(x.ab[r], pg, s.ch);
+    }
+    s.w0 = (uint64_t)__popc(W1) | ((uint64_t)__dp4a(W1, x.Q, 0u) << 16) | ((uint64_t)__dp4a(W1, x.D, 0u) << 39);
+    return s;
+}
+
 // --- local_mem (src/kernels/ht_in_local_mem.cuh:11-74): per-thread tables indexed by the row's
 // group, which places them in (L1-cached) local memory. A group's entry is four 64-bit words
 // (five for reference-typed columns, whose quantity needs a word of its own): the count, quantity
-// and discount share one word, since a thread adds at most 2^15 rows per launch
-// (count < 2^16, quantity <= 255 * 2^15 < 2^23, discount <= 100 * 2^15 < 2^22), then price,
-// (100 - d) price and (100 - d)(100 + t) price. A row is one read-modify-write per word.
+// and discount share one word (see quad_group_sums), then price, (100 - d) price and
+// (100 - d)(100 + t) price. Compressed quads are added group by group, every lane of the warp at
+// the same group at a time: the group's four rows are summed in registers and its entry is
+// read and written once, by accesses that coalesce across the warp (a row-by-row update at each
+// row's own group scatters the warp's accesses over the table: 2.8 sectors per row each way,
+// L1-bound). Reference-typed rows come one at a time and update their group's entry.
 template <int G, bool kWideQty>
 struct AccLocal {
     static constexpr int kWords = kWideQty ? 5 : 4;
@@ -383,9 +406,18 @@ struct AccLocal {
         }
     }
     __device__ __forceinline__ void add_quad(const Quad& x) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-            add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
+        // not unrolled, so that the table stays in local memory, indexed by the loop's group
+#pragma unroll 1
+        for (int g = 0; g < G; ++g) {
+            const uint32_t W1 = (x.OH >> g) & 0x01010101u;
+            if (W1) {
+                const QuadGroupSums q = quad_group_sums(W1, x);
+                t[g][0] += q.w0;
+                t[g][1] += q.p;
+                t[g][2] += q.dp;
+                t[g][3] += q.ch;
+            }
+        }
     }
     __device__ __forceinline__ void fold() {}
     __device__ __forceinline__ bool owns(uint32_t) const { return true; }
@@ -410,37 +442,51 @@ struct AccLocal {
 };
 
 // --- shared_mem_per_thread (src/kernels/ht_in_shared_mem_per_thread.cuh:23-118): per-thread
-// tables in shared memory, laid out [field][group][thread] so a warp's accesses are
-// bank-conflict free.
+// tables in shared memory, laid out [word][group][thread] so a warp's accesses are bank-conflict
+// free. A group's entry holds the same words as the local_mem table, and compressed quads are
+// added group by group in the same way: every lane at the same group, one read-modify-write per
+// word and group.
 template <int G, bool kWideQty>
 struct AccSharedPerThread {
-    uint64_t* tab;       // 5 * G * T entries
-    uint32_t* cnt;       // G * T entries
+    static constexpr int kWords = kWideQty ? 5 : 4;
+    static constexpr int kDiscShift = kWideQty ? 16 : 39;
+    uint64_t* tab;       // kWords * G * T entries: [w0, p, dp, ch, (quantity)][group][thread]
     uint32_t tid, nthreads;
     __device__ __forceinline__ void init(uint32_t, uint32_t consumer_tid, uint8_t* scratch) {
         tid = consumer_tid;
         nthreads = blockDim.x - 32;
         tab = reinterpret_cast<uint64_t*>(scratch);
-        cnt = reinterpret_cast<uint32_t*>(tab + 5 * G * nthreads);
-        for (int i = 0; i < 5 * G; ++i) tab[i * nthreads + tid] = 0;
-        for (int i = 0; i < G; ++i) cnt[i * nthreads + tid] = 0;
+        for (int i = 0; i < kWords * G; ++i) tab[i * nthreads + tid] = 0;
     }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
         if (c < (uint32_t)G) {
             const uint32_t base = c * nthreads + tid;
             const uint32_t stride = G * nthreads;
-            tab[base] += p;
-            tab[base + stride] = mad_wide(a, p, tab[base + stride]);
-            tab[base + 2 * stride] = mad_wide(ab, p, tab[base + 2 * stride]);
-            tab[base + 3 * stride] += q;
-            tab[base + 4 * stride] += d;
-            cnt[base] += 1;
+            if constexpr (kWideQty) {
+                tab[base] += 1ull | ((uint64_t)d << kDiscShift);
+                tab[base + 4 * stride] += q;
+            } else {
+                tab[base] += 1ull | ((uint64_t)q << 16) | ((uint64_t)d << kDiscShift);
+            }
+            tab[base + stride] += p;
+            tab[base + 2 * stride] = mad_wide(a, p, tab[base + 2 * stride]);
+            tab[base + 3 * stride] = mad_wide(ab, p, tab[base + 3 * stride]);
         }
     }
     __device__ __forceinline__ void add_quad(const Quad& x) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-            add(quad_code(x, r), (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r], x.ab[r], x.p[r]);
+        const uint32_t stride = G * nthreads;
+#pragma unroll 1
+        for (int g = 0; g < G; ++g) {
+            const uint32_t W1 = (x.OH >> g) & 0x01010101u;
+            if (W1) {
+                const QuadGroupSums q = quad_group_sums(W1, x);
+                const uint32_t base = g * nthreads + tid;
+                tab[base] += q.w0;
+                tab[base + stride] += q.p;
+                tab[base + 2 * stride] += q.dp;
+                tab[base + 3 * stride] += q.ch;
+            }
+        }
     }
     __device__ __forceinline__ void fold() {}
     // whether this thread sums the rows of group code c (every thread reads every row it is given)
@@ -454,8 +500,10 @@ struct AccSharedPerThread {
 #pragma unroll
         for (int i = 0; i < G; ++i) {
             const uint32_t base = i * nthreads + tid;
-            const uint64_t vals[kNumAggs] = {cnt[base], tab[base + 3 * stride], tab[base], tab[base + 4 * stride],
-                                             tab[base + stride], tab[base + 2 * stride]};
+            const uint64_t w0 = tab[base];
+            const uint64_t qty = kWideQty ? tab[base + 4 * stride] : (w0 >> 16) & ((1ull << 23) - 1);
+            const uint64_t vals[kNumAggs] = {w0 & 0xFFFFull, qty, tab[base + stride], w0 >> kDiscShift,
+                                             tab[base + 2 * stride], tab[base + 3 * stride]};
 #pragma unroll
             for (int a = 0; a < kNumAggs; ++a) {
                 uint64_t lo = vals[a], hi = 0;
@@ -860,7 +908,7 @@ static cudaError_t launch_one(const ScanParams& prm, int sm_count, int max_block
     constexpr uint32_t W = kConsumerWarps;
     constexpr int G = LayoutTraits<L>::kCodes;
     uint32_t dyn = S * stage_bytes<L>(R);
-    if (P == kPlaceSharedMemPerThread) dyn += (uint32_t)(44 * G * W * 32);
+    if (P == kPlaceSharedMemPerThread) dyn += (uint32_t)(8 * (L == kLayUncomp ? 5 : 4) * G * W * 32);
     cudaError_t e = cudaFuncSetAttribute(q1_scan_kernel<L, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = scan_grid_blocks(L, prm.rows, sm_count, max_blocks);
