@@ -18,6 +18,8 @@ SEED = 808
 def test_inject_fault_argument_checks():
     L = q.lib()
     assert L.q1_inject_fault(0, 0) == 0
+    assert L.q1_inject_fault(4, 0) == 0
+    assert L.q1_inject_fault(5, 1) == 1
     assert L.q1_inject_fault(99, 1) == 1
     assert L.q1_selftest_wait_timeout(0, None) == 1
 
@@ -70,3 +72,44 @@ def test_allocation_faults_are_reported_and_recoverable(cuda, kind, residency):
         with q.Q1Context() as ref:
             ref.generate(SEED, ROWS, layout="compressed", packing="pair", residency=residency)
             assert np.array_equal(r.table(), ref.run(apply_compression=True, num_query_execution_runs=1).table())
+
+
+@pytest.mark.gpu
+def test_failed_serving_round_fails_what_follows_and_server_reopens(cuda):
+    """A serving round that fails (injected on the host while another round lane may be busy)
+    fails its own requests, the rounds queued behind it and every request still waiting; the server
+    then refuses submissions, closes cleanly, and a new server on the same device answers exactly."""
+    from test_gpu_serve import ADHOC, FLAGS, KEYS, RES, open_server, plain, req, submit, words
+    L = q.lib()
+    h = open_server(slots=4, lanes=2)
+    try:
+        r0 = req(ADHOC, KEYS, 729999, 9, 300_000, 7)
+        ok = _lib.Response()
+        assert L.q1_server_wait(h, submit(h, r0), 60_000, ctypes.byref(ok)) == 0
+        _lib.check(L.q1_inject_fault(4, 1))   # Q1_FAULT_SERVE_ROUND: the next round fails to enqueue
+        reqs = [req(ADHOC, KEYS, 729990 + i, 9, 300_000, 7) if i % 2 else req(RES, FLAGS, 729950 + i)
+                for i in range(24)]
+        tickets = [submit(h, r) for r in reqs]
+        statuses = []
+        for t in tickets:
+            resp = _lib.Response()
+            statuses.append(L.q1_server_wait(h, t, 60_000, ctypes.byref(resp)))
+            assert resp.status == statuses[-1]
+        assert 10 in statuses, statuses                       # Q1_ERR_INTERNAL
+        first = statuses.index(10)
+        assert all(s == 0 for s in statuses[:first]) and all(s == 10 for s in statuses[first:]), statuses
+        t = ctypes.c_uint64()
+        assert L.q1_server_submit(h, ctypes.byref(r0), ctypes.byref(t)) == 10
+        st = _lib.ServerStats()
+        _lib.check(L.q1_server_stats_get(h, ctypes.byref(st)))
+        assert st.failed == len(reqs) - first and st.pending == 0
+    finally:
+        _lib.check(L.q1_server_close(h))
+    h2 = open_server(slots=4, lanes=2)
+    try:
+        resp = _lib.Response()
+        assert L.q1_server_wait(h2, submit(h2, r0), 60_000, ctypes.byref(resp)) == 0
+        assert np.array_equal(words(resp), words(plain(h2, r0)))
+        assert np.array_equal(words(resp), words(ok))
+    finally:
+        _lib.check(L.q1_server_close(h2))

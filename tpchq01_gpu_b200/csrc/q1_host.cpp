@@ -639,7 +639,7 @@ q1_status q1_inject_fault(q1_fault kind, uint32_t count) {
         for (int k = 1; k < kFaultKinds; ++k) set_faults(k, 0);
         return Q1_OK;
     }
-    if (kind < Q1_FAULT_CPU_WORKER || kind > Q1_FAULT_PINNED_ALLOC)
+    if (kind < Q1_FAULT_CPU_WORKER || kind > Q1_FAULT_SERVE_ROUND)
         return set_error(Q1_ERR_INVALID_ARGUMENT, "unknown fault kind");
     set_faults((int)kind, count);
     return Q1_OK;

@@ -57,7 +57,8 @@ uint64_t words32(uint64_t rows);   // 1-bit containers
 // ------------------------------------------------------------------------------------------
 
 // Host-side fault injection (q1_inject_fault): the next `count` events of a kind fail.
-enum FaultKind : int { kFaultCpuWorker = 1, kFaultDeviceAlloc = 2, kFaultPinnedAlloc = 3, kFaultKinds = 4 };
+enum FaultKind : int { kFaultCpuWorker = 1, kFaultDeviceAlloc = 2, kFaultPinnedAlloc = 3, kFaultServeRound = 4,
+                       kFaultKinds = 5 };
 bool take_fault(FaultKind kind);   // consumes one pending fault of `kind`, if any
 void set_faults(int kind, uint32_t count);
 

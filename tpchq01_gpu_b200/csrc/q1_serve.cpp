@@ -748,7 +748,10 @@ void dispatcher_loop(q1_server* s) {
             if (!s->inflight.empty()) s->overlapped_rounds++;
             s->max_in_flight = std::max<uint32_t>(s->max_in_flight, (uint32_t)s->inflight.size() + 1);
         }
-        Ln->enq = s->opts.mode == Q1_SERVE_PLAIN ? enqueue_plain(s, Ln) : enqueue_round(s, Ln);
+        if (take_fault(kFaultServeRound))
+            Ln->enq = set_error(Q1_ERR_INTERNAL, "injected serving round failure");
+        else
+            Ln->enq = s->opts.mode == Q1_SERVE_PLAIN ? enqueue_plain(s, Ln) : enqueue_round(s, Ln);
         Ln->err = Ln->enq == Q1_OK ? std::string() : std::string(q1_last_error());
         std::lock_guard<std::mutex> lk(s->m);
         s->inflight.push_back(Ln);
