@@ -8,25 +8,27 @@
 //   PlaneRegs<NG>  num_groups <= NG (4 or 8): per-thread byte-plane dot products (dp4a), four
 //                  rows per instruction, as in the scan kernel; no atomics until a flush.
 //   Cube3Table     num_groups <= 64: a shared-memory table per (group, discount, tax) cell; a
-//                  row adds its count and quantity (one packed word) and its price: two atomics.
+//                  row adds its count, its quantity and its price: three atomics.
 //   CubeTable      num_groups <= 1024: a shared-memory table per (group, discount) cell. A row
-//                  adds only its count and quantity (one packed word), its price and tax * price;
-//                  the discounted sums follow exactly at the flush, because the discount of a
-//                  cell is known there: sum (100-d) p = sum_d (100-d) P_d and
+//                  adds its count, price and tax * price to its cell and its quantity to its
+//                  group's word; the discounted sums follow exactly at the flush, because the
+//                  discount of a cell is known there: sum (100-d) p = sum_d (100-d) P_d and
 //                  sum (100-d)(100+t) p = sum_d (100-d) (100 P_d + TP_d).
 //   SlotTable      one shared-memory slot per key below the table's size (2048 in the batch
-//                  kernel, 4096 in the group-key kernel and the partitioned path): count and
-//                  discount packed, quantity, price, disc_price, charge.
+//                  kernel, 4096 in the group-key kernel and the partitioned path): count,
+//                  discount, quantity, price, disc_price, charge.
 //   global         every row reduces straight into the scratch accumulators.
 // The shared tables use only 32-bit shared atomics (64-bit shared atomics are far slower).
-// The slot table and the (group, discount, tax) cube keep 64-bit sums as (low word, carry word)
-// pairs: the low word's atomic returns the old value, and a wrap adds the carry to the high word.
-// The (group, discount) cube keeps only the low words of its cells, so that 1024 groups fit: a
-// wrap of a cell's packed count-plus-quantity word (about one row in ten) counts in a shared
-// word per group, worth 2^8 units of quantity; a wrap of a price or tax-price word (a few rows in
-// a thousand) adds its 2^32 straight to the group's scratch sums, where the cell's discount fixes
-// what it is worth in each. (The same scheme in the (group, discount, tax) cube measured 3%
-// slower at 64 groups, whose per-group words the frequent quantity wraps contend for.) Rows
+// Counts and quantities cannot wrap a 32-bit word between two flushes (at most 2^23 rows per
+// CTA: count < 2^24, quantity <= 255 * 2^23 < 2^32), so their atomics need no result and no carry
+// check. (Packing a count and 2^24 x its quantity into one word saved an atomic but wrapped about
+// every tenth row of a cell, so the warp-voted carry branch ran on nearly every quad: 11.7 shared
+// atomic instructions per warp and quad where 8 were needed.) Price sums can wrap: the slot table
+// and the (group, discount, tax) cube keep them as (low word, carry word) pairs: the low word's
+// atomic returns the old value, and a wrap adds the carry to the high word. The
+// (group, discount) cube keeps only the low words of its cells, so that 1024 groups fit: a wrap of
+// a price or tax-price word (a few rows in a thousand) adds its 2^32 straight to the group's
+// scratch sums, where the cell's discount fixes what it is worth in each. Rows
 // outside the tables' fast domain
 // (discount > 10, tax > 8 or price >= 2^24; TPC-H data has none) take the global path, so every
 // result is exact over the whole compressed domain.
@@ -67,14 +69,14 @@ constexpr uint64_t kTableFlushRows = 1ull << 23;
 
 constexpr uint32_t kCubeMaxGroups = 1024;
 constexpr uint32_t kCubeDisc = 11;          // discount 0..10
-constexpr uint32_t kCubeWords = 3;          // x p t (low words)
+constexpr uint32_t kCubeWords = 3;          // count, price, tax * price (low words)
 constexpr uint32_t kCube3MaxGroups = 64;
 constexpr uint32_t kCubeTax = 9;            // tax 0..8
-constexpr uint32_t kCube3Words = 4;         // xlo xhi plo phi
+constexpr uint32_t kCube3Words = 4;         // count, quantity, price low, price carry
 constexpr uint32_t kSlots = 2048;
-constexpr uint32_t kSlotWords = 9;          // xlo xhi q plo phi dlo dhi clo chi
+constexpr uint32_t kSlotWords = 9;          // count, discount, quantity, price lo/hi, disc_price lo/hi, charge lo/hi
 
-// cells, then (CubeTable) one word per group for the wraps of its count-plus-quantity words
+// cells, then (CubeTable) one quantity word per group
 __host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) {
     return num_groups * (kCubeDisc * kCubeWords + 1) * 4;
 }
@@ -239,13 +241,13 @@ struct PlaneRegs {
 // CubeTable: shared (group, discount) cells
 // ---------------------------------------------------------------------------------------------
 struct CubeTable {
-    uint32_t* w;       // [kCubeWords][cells]: count + 2^24 quantity, price, tax * price
-    uint32_t* qc;      // [groups]: wraps of the groups' count-plus-quantity words
+    uint32_t* w;       // [kCubeWords][cells]: count, price, tax * price
+    uint32_t* qg;      // [groups]: quantity
     uint32_t cells;
     __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
         w = reinterpret_cast<uint32_t*>(base);
         cells = num_groups * kCubeDisc;
-        qc = w + kCubeWords * cells;
+        qg = w + kCubeWords * cells;
     }
     __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
         for (uint32_t i = tid; i < kCubeWords * cells + cells / kCubeDisc; i += nthreads) w[i] = 0;
@@ -254,19 +256,21 @@ struct CubeTable {
     // atomics of the quad are issued before any carry is checked, so their latencies overlap.
     static constexpr bool kPacked = true;
     // The quantity, discount and tax bytes of the four rows packed in Q, D, X; acc: the scratch
-    // that takes the price words' wraps.
+    // that takes the price words' wraps. A cell's count and a group's quantity cannot wrap
+    // between flushes (at most 2^23 rows per CTA: count < 2^24, quantity <= 255 * 2^23 < 2^32),
+    // so their atomics need no result.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
                                                     uint32_t X, const uint32_t p[4], unsigned long long* acc) {
-        uint32_t c[4], vx[4], vt[4], ox[4], op[4], ot[4];
+        uint32_t c[4], vt[4], op[4], ot[4];
         if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             c[r] = key[r] * kCubeDisc + ((D >> (8 * r)) & 0xFFu);
-            vx[r] = __byte_perm(Q, 1u, 0x0554u | ((uint32_t)r << 12));   // count + 2^24 * quantity
             vt[r] = ((X >> (8 * r)) & 0xFFu) * p[r];                     // t p < 2^28
-            ox[r] = op[r] = ot[r] = 0;
+            op[r] = ot[r] = 0;
             if ((m >> r) & 1u) {
-                ox[r] = atomicAdd(w + c[r], vx[r]);
+                atomicAdd(w + c[r], 1u);
+                atomicAdd(qg + key[r], (Q >> (8 * r)) & 0xFFu);
                 op[r] = atomicAdd(w + cells + c[r], p[r]);
                 ot[r] = atomicAdd(w + 2 * cells + c[r], vt[r]);
             }
@@ -275,12 +279,11 @@ struct CubeTable {
         // the rows only in the rare branch
         bool wrap = false;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) wrap |= (ox[r] > ~vx[r]) | (op[r] > ~p[r]) | (ot[r] > ~vt[r]);
+        for (int r = 0; r < 4; ++r) wrap |= (op[r] > ~p[r]) | (ot[r] > ~vt[r]);
         if (__any_sync(0xffffffffu, wrap)) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const uint32_t a = 100u - ((D >> (8 * r)) & 0xFFu);
-                if (ox[r] > ~vx[r]) atomicAdd(qc + key[r], 1u);
                 if (op[r] > ~p[r]) carry_price(acc, key[r], a, 100u * a);
                 if (ot[r] > ~vt[r]) red_add(acc + 8ull * key[r] + 7, a);
             }
@@ -289,16 +292,14 @@ struct CubeTable {
     // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
     __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t tid, uint32_t nthreads) {
         for (uint32_t g = tid; g < num_groups; g += nthreads) {
-            uint64_t cnt = 0, q = (uint64_t)qc[g] << 8, dsum = 0, P = 0;
+            uint64_t cnt = 0, q = qg[g], dsum = 0, P = 0;
             unsigned __int128 DP = 0, CH = 0;
-            qc[g] = 0;
+            qg[g] = 0;
 #pragma unroll
             for (uint32_t d = 0; d < kCubeDisc; ++d) {
                 const uint32_t c = g * kCubeDisc + d;
-                const uint32_t X = w[c], Pd = w[cells + c], TPd = w[2 * cells + c];
-                const uint32_t nd = X & 0xFFFFFFu;
+                const uint32_t nd = w[c], Pd = w[cells + c], TPd = w[2 * cells + c];
                 cnt += nd;
-                q += X >> 24;
                 dsum += (uint64_t)d * nd;
                 P += Pd;
                 DP += (uint64_t)(100u - d) * Pd;
@@ -315,11 +316,12 @@ struct CubeTable {
 
 // ---------------------------------------------------------------------------------------------
 // Cube3Table: shared (group, discount, tax) cells, for num_groups <= 64. A row adds only its
-// count and quantity (one packed word) and its price: two atomics. At the flush the cell's
-// discount and tax give sum (100-d) p = (100-d) P and sum (100-d)(100+t) p = (100-d)(100+t) P.
+// count, quantity and price: three atomics, of which only the price's can wrap (into the cell's
+// carry word) between flushes. At the flush the cell's discount and tax give
+// sum (100-d) p = (100-d) P and sum (100-d)(100+t) p = (100-d)(100+t) P.
 // ---------------------------------------------------------------------------------------------
 struct Cube3Table {
-    uint32_t* w;       // [kCube3Words][cells]
+    uint32_t* w;       // [kCube3Words][cells]: count, quantity, price low word, price carry word
     uint32_t cells;
     __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
         w = reinterpret_cast<uint32_t*>(base);
@@ -334,31 +336,29 @@ struct Cube3Table {
     // 9 d + t < 99 fits a byte, so one shift-and-add gives the four (discount, tax) cell offsets.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
                                                     uint32_t X, const uint32_t p[4], unsigned long long*) {
-        uint32_t c[4], vx[4], ox[4], op[4];
+        uint32_t c[4], op[4];
         if (!__any_sync(0xffffffffu, m)) return;
         const uint32_t DT = (D << 3) + D + X;   // bytes r: 9 d + t (garbage outside the fast domain)
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             c[r] = key[r] * (kCubeDisc * kCubeTax) + ((DT >> (8 * r)) & 0xFFu);
-            vx[r] = __byte_perm(Q, 1u, 0x0554u | ((uint32_t)r << 12));   // count + 2^24 * quantity
-            ox[r] = op[r] = 0;
+            op[r] = 0;
             if ((m >> r) & 1u) {
-                ox[r] = atomicAdd(w + c[r], vx[r]);
+                atomicAdd(w + c[r], 1u);
+                atomicAdd(w + cells + c[r], (Q >> (8 * r)) & 0xFFu);
                 op[r] = atomicAdd(w + 2 * cells + c[r], p[r]);
             }
         }
-        // a word wrapped iff old > ~added (rows not added have old == 0): one predicate and
-        // one vote, the rows only in the branch (the count-plus-quantity word wraps about every
-        // tenth row of a cell, the price word every few hundred)
+        // a price word wrapped iff old > ~added (rows not added have old == 0): one predicate
+        // and one vote, the rows only in the branch (a cell's price word wraps every thousand
+        // rows or so; its count and quantity words cannot wrap between flushes)
         bool wrap = false;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) wrap |= (ox[r] > ~vx[r]) | (op[r] > ~p[r]);
+        for (int r = 0; r < 4; ++r) wrap |= op[r] > ~p[r];
         if (__any_sync(0xffffffffu, wrap)) {
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                if (ox[r] > ~vx[r]) atomicAdd(w + cells + c[r], 1u);
+            for (int r = 0; r < 4; ++r)
                 if (op[r] > ~p[r]) atomicAdd(w + 3 * cells + c[r], 1u);
-            }
         }
     }
     // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
@@ -372,10 +372,9 @@ struct Cube3Table {
 #pragma unroll
                 for (uint32_t t = 0; t < kCubeTax; ++t) {
                     const uint32_t c = (g * kCubeDisc + d) * kCubeTax + t;
-                    const uint64_t X = ((uint64_t)w[cells + c] << 32) | w[c];
                     const uint64_t Pt = ((uint64_t)w[3 * cells + c] << 32) | w[2 * cells + c];
-                    cd += X & 0xFFFFFFull;
-                    q += X >> 24;
+                    cd += w[c];
+                    q += w[cells + c];
                     Pd += Pt;
                     Td += (unsigned __int128)(100u + t) * Pt;
 #pragma unroll
@@ -413,20 +412,20 @@ struct SlotTable {
     __device__ __forceinline__ void add_quad(uint32_t m, const uint32_t key[4], const uint32_t q[4],
                                              const uint32_t d[4], const uint32_t t[4], const uint32_t p[4]) {
         const uint32_t S = slots;
-        uint32_t vx[4], vd[4], cl[4], ch[4], ox[4], op[4], od[4], oc[4];
+        uint32_t vd[4], cl[4], ch[4], op[4], od[4], oc[4];
         if (!__any_sync(0xffffffffu, m)) return;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const uint32_t a = 100u - d[r];
-            vx[r] = 1u + (d[r] << 24);   // count + 2^24 * discount
             vd[r] = a * p[r];            // (100 - d) p < 2^31
             const uint64_t c64 = (uint64_t)(a * (100u + t[r])) * p[r];
             cl[r] = (uint32_t)c64;
             ch[r] = (uint32_t)(c64 >> 32);
-            ox[r] = op[r] = od[r] = oc[r] = 0;
+            op[r] = od[r] = oc[r] = 0;
             if ((m >> r) & 1u) {
                 const uint32_t s = key[r];
-                ox[r] = atomicAdd(w + s, vx[r]);
+                atomicAdd(w + s, 1u);
+                atomicAdd(w + S + s, d[r]);
                 atomicAdd(w + 2 * S + s, q[r]);
                 op[r] = atomicAdd(w + 3 * S + s, p[r]);
                 od[r] = atomicAdd(w + 5 * S + s, vd[r]);
@@ -438,7 +437,7 @@ struct SlotTable {
         bool wrap = false;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            wrap |= (ox[r] > ~vx[r]) | (op[r] > ~p[r]) | (od[r] > ~vd[r]);
+            wrap |= (op[r] > ~p[r]) | (od[r] > ~vd[r]);
             ch[r] = ((m >> r) & 1u) ? ch[r] + (oc[r] > ~cl[r] ? 1u : 0u) : 0u;
         }
         // the charge's high word is nonzero for most rows: added per row
@@ -448,7 +447,6 @@ struct SlotTable {
         if (__any_sync(0xffffffffu, wrap)) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                if (ox[r] > ~vx[r]) atomicAdd(w + S + key[r], 1u);
                 if (op[r] > ~p[r]) atomicAdd(w + 4 * S + key[r], 1u);
                 if (od[r] > ~vd[r]) atomicAdd(w + 6 * S + key[r], 1u);
             }
@@ -457,11 +455,10 @@ struct SlotTable {
     __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t tid, uint32_t nthreads) {
         const uint32_t S = slots;
         for (uint32_t s = tid; s < S; s += nthreads) {
-            const uint64_t X = ((uint64_t)w[S + s] << 32) | w[s];
-            const uint64_t cnt = X & 0xFFFFFFull;
+            const uint64_t cnt = w[s];
             if (cnt) {
                 const uint64_t P = ((uint64_t)w[4 * S + s] << 32) | w[3 * S + s];
-                scratch_add(acc, s, cnt, w[2 * S + s], X >> 24, P, w[5 * S + s], w[6 * S + s], w[7 * S + s],
+                scratch_add(acc, s, cnt, w[2 * S + s], w[S + s], P, w[5 * S + s], w[6 * S + s], w[7 * S + s],
                             w[8 * S + s]);
             }
 #pragma unroll
