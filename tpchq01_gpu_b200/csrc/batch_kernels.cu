@@ -53,6 +53,8 @@ constexpr uint32_t kKindFull = 0, kKindPartial = 1, kKindEnd = 2;
 constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 constexpr uint32_t kTableBytes =
     cmax(ka::cube3_bytes(ka::kCube3MaxGroups), cmax(ka::cube_bytes(ka::kCubeMaxGroups), ka::slot_bytes(ka::kSlots)));
+// the table kernel's ring and table, with room left for its static shared memory (< 1 KB)
+static_assert(3 * kStage + kTableBytes + 512 <= 227 * 1024, "table kernel shared memory");
 
 struct __align__(16) StageMeta {
     uint32_t instance;

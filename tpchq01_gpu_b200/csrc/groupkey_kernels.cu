@@ -77,6 +77,10 @@ __host__ __device__ constexpr uint32_t table_bytes(uint32_t kind, uint32_t num_g
 __host__ __device__ constexpr uint32_t ring_stages(uint32_t kind, uint32_t num_groups) {
     return kMaxStages * ka::kStageBytes + table_bytes(kind, num_groups) <= kMaxDynSmem ? kMaxStages : kMaxStages - 1;
 }
+// the largest tables fit beside a 3-stage ring, with room left for the static shared memory
+static_assert((kMaxStages - 1) * ka::kStageBytes + ka::cube_bytes(ka::kCubeMaxGroups) + 512 <= kMaxDynSmem,
+              "1024-group cells");
+static_assert((kMaxStages - 1) * ka::kStageBytes + ka::slot_bytes(kWideSlots) + 512 <= kMaxDynSmem, "slot table");
 
 }  // namespace gk
 

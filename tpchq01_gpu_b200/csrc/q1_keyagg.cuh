@@ -10,13 +10,14 @@
 //   Cube3Table     num_groups <= 64: a shared-memory table per (group, discount, tax) cell; a
 //                  row adds its count, its quantity and its price: three atomics.
 //   CubeTable      num_groups <= 1024: a shared-memory table per (group, discount) cell. A row
-//                  adds its count, price and tax * price to its cell and its quantity to its
-//                  group's word; the discounted sums follow exactly at the flush, because the
+//                  adds its count, price and tax * price to its cell and its quantity to one of
+//                  its group's four words; the discounted sums follow exactly at the flush, because the
 //                  discount of a cell is known there: sum (100-d) p = sum_d (100-d) P_d and
 //                  sum (100-d)(100+t) p = sum_d (100-d) (100 P_d + TP_d).
 //   SlotTable      one shared-memory slot per key below the table's size (2048 in the batch
 //                  kernel, 4096 in the group-key kernel and the partitioned path): count,
-//                  discount, quantity, price, disc_price, charge.
+//                  discount, quantity, price, discount x price, charge; disc_price follows at
+//                  the flush as 100 sum p - sum d p.
 //   global         every row reduces straight into the scratch accumulators.
 // The shared tables use only 32-bit shared atomics (64-bit shared atomics are far slower).
 // Counts and quantities cannot wrap a 32-bit word between two flushes (at most 2^23 rows per
@@ -74,11 +75,12 @@ constexpr uint32_t kCube3MaxGroups = 64;
 constexpr uint32_t kCubeTax = 9;            // tax 0..8
 constexpr uint32_t kCube3Words = 4;         // count, quantity, price low, price carry
 constexpr uint32_t kSlots = 2048;
-constexpr uint32_t kSlotWords = 9;          // count, discount, quantity, price lo/hi, disc_price lo/hi, charge lo/hi
+constexpr uint32_t kSlotWords = 9;          // count, discount, quantity, price lo/hi, discount x price lo/hi, charge lo/hi
 
-// cells, then (CubeTable) one quantity word per group
+// cells, then (CubeTable) kCubeQtyWays quantity words per group
+constexpr uint32_t kCubeQtyWays = 4;
 __host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) {
-    return num_groups * (kCubeDisc * kCubeWords + 1) * 4;
+    return num_groups * (kCubeDisc * kCubeWords + kCubeQtyWays) * 4;
 }
 __host__ __device__ constexpr uint32_t cube3_bytes(uint32_t num_groups) {
     return num_groups * kCubeDisc * kCubeTax * kCube3Words * 4;
@@ -242,7 +244,8 @@ struct PlaneRegs {
 // ---------------------------------------------------------------------------------------------
 struct CubeTable {
     uint32_t* w;       // [kCubeWords][cells]: count, price, tax * price
-    uint32_t* qg;      // [groups]: quantity
+    uint32_t* qg;      // [groups][kCubeQtyWays]: quantity, a row's in word (discount & 3), so that the
+                       // rows of a frequent key spread their atomics over four words
     uint32_t cells;
     __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
         w = reinterpret_cast<uint32_t*>(base);
@@ -250,7 +253,7 @@ struct CubeTable {
         qg = w + kCubeWords * cells;
     }
     __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
-        for (uint32_t i = tid; i < kCubeWords * cells + cells / kCubeDisc; i += nthreads) w[i] = 0;
+        for (uint32_t i = tid; i < kCubeWords * cells + kCubeQtyWays * (cells / kCubeDisc); i += nthreads) w[i] = 0;
     }
     // Rows r of a quad with bit r of `m` set (passing, key < num_groups, fast domain). All
     // atomics of the quad are issued before any carry is checked, so their latencies overlap.
@@ -270,7 +273,7 @@ struct CubeTable {
             op[r] = ot[r] = 0;
             if ((m >> r) & 1u) {
                 atomicAdd(w + c[r], 1u);
-                atomicAdd(qg + key[r], (Q >> (8 * r)) & 0xFFu);
+                atomicAdd(qg + key[r] * kCubeQtyWays + ((D >> (8 * r)) & 3u), (Q >> (8 * r)) & 0xFFu);
                 op[r] = atomicAdd(w + cells + c[r], p[r]);
                 ot[r] = atomicAdd(w + 2 * cells + c[r], vt[r]);
             }
@@ -292,9 +295,13 @@ struct CubeTable {
     // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
     __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t tid, uint32_t nthreads) {
         for (uint32_t g = tid; g < num_groups; g += nthreads) {
-            uint64_t cnt = 0, q = qg[g], dsum = 0, P = 0;
+            uint64_t cnt = 0, q = 0, dsum = 0, P = 0;
             unsigned __int128 DP = 0, CH = 0;
-            qg[g] = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < kCubeQtyWays; ++j) {
+                q += qg[g * kCubeQtyWays + j];
+                qg[g * kCubeQtyWays + j] = 0;
+            }
 #pragma unroll
             for (uint32_t d = 0; d < kCubeDisc; ++d) {
                 const uint32_t c = g * kCubeDisc + d;
@@ -417,7 +424,7 @@ struct SlotTable {
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const uint32_t a = 100u - d[r];
-            vd[r] = a * p[r];            // (100 - d) p < 2^31
+            vd[r] = d[r] * p[r];         // d p < 2^28 (the discounted price follows at the flush)
             const uint64_t c64 = (uint64_t)(a * (100u + t[r])) * p[r];
             cl[r] = (uint32_t)c64;
             ch[r] = (uint32_t)(c64 >> 32);
@@ -458,7 +465,8 @@ struct SlotTable {
             const uint64_t cnt = w[s];
             if (cnt) {
                 const uint64_t P = ((uint64_t)w[4 * S + s] << 32) | w[3 * S + s];
-                scratch_add(acc, s, cnt, w[2 * S + s], w[S + s], P, w[5 * S + s], w[6 * S + s], w[7 * S + s],
+                const uint64_t DP = 100u * P - (((uint64_t)w[6 * S + s] << 32) | w[5 * S + s]);   // sum (100 - d) p
+                scratch_add(acc, s, cnt, w[2 * S + s], w[S + s], P, DP & 0xFFFFFFFFull, DP >> 32, w[7 * S + s],
                             w[8 * S + s]);
             }
 #pragma unroll
