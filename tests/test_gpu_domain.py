@@ -165,14 +165,16 @@ def test_uncompressed_wide_values_summed_exactly(cuda, wide_unc, placement):
     assert np.array_equal(read(buf), want)
 
 
+@pytest.mark.parametrize("residency", ["hbm", "pinned"])
 @pytest.mark.parametrize("fraction", [0.0, 0.4])
-def test_uncompressed_wide_values_through_q1_run(cuda, wide_unc, fraction):
-    """The same rows through q1_run, GPU alone and with the CPU share of coprocessing."""
+def test_uncompressed_wide_values_through_q1_run(cuda, wide_unc, fraction, residency):
+    """The same rows through q1_run, HBM-resident and streamed from pinned host memory, GPU alone
+    and with the CPU share of coprocessing."""
     want, _ = O.q1_uncompressed(wide_unc, CUTOFF)
     with q.Q1Context(cpu_threads=3) as ctx:
-        ctx.load_columns(wide_unc, "uncompressed", "pair", "hbm")
+        ctx.load_columns(wide_unc, "uncompressed", "pair", residency)
         res = ctx.run(apply_compression=False, use_coprocessing=fraction > 0, cpu_processing_fraction=fraction,
-                      num_query_execution_runs=1)
+                      num_tuples_per_kernel_launch=1 << 16, num_query_execution_runs=1)
     assert np.array_equal(res.table(), want)
 
 
