@@ -318,8 +318,10 @@ q1_status q1_launch_compressed(q1_placement placement, const q1_compressed_colum
  * 147,712 bytes that every GPU loading the library holds until exit: a status word plus one
  * partial-sum record per CTA, which a second kernel adds into dev_aggregates (accumulating, like
  * q1_launch_compressed). Limit: at most 256 CTAs per launch (one per SM is used by default, 148
- * on a B200); larger grids are rejected with Q1_ERR_INVALID_ARGUMENT. The first call on a device
- * looks up the array's address (cudaGetSymbolAddress). The call is synchronous: it waits for
+ * on a B200); larger grids are rejected with Q1_ERR_INVALID_ARGUMENT. The first call on a device,
+ * and the first after that device's context was reset, looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. The call is
+ * synchronous: it waits for
  * `cuda_stream` and returns Q1_ERR_DOMAIN / Q1_ERR_DEVICE_TIMEOUT itself. All calls share the
  * array, so calls whose GPU work overlaps (other threads or streams of the same device) race. */
 q1_status q1_launch_compressed_noalloc(q1_placement placement, const q1_compressed_columns* dev_cols,

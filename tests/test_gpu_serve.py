@@ -230,6 +230,16 @@ def test_rejections(server):
     assert L.q1_server_wait(server, 123456789, 0, ctypes.byref(_lib.Response())) == 1
 
 
+def test_round_lane_option_is_checked(cuda):
+    o = _lib.ServerOpts()
+    q.lib().q1_server_opts_default(ctypes.byref(o))
+    assert o.max_rounds_in_flight == 2
+    o.max_rounds_in_flight = 9
+    h = ctypes.c_void_p()
+    assert q.lib().q1_server_open(ctypes.byref(o), ctypes.byref(h)) == 1   # Q1_ERR_INVALID_ARGUMENT
+    assert not h.value
+
+
 def test_budget_refusal(cuda):
     h = open_server(budget=1 << 20, slots=4)
     try:
