@@ -627,23 +627,44 @@ __device__ __forceinline__ void process_step(const ScanParams& prm, uint32_t bas
         const uint4 P = lds_v4(base + col_offset<L>(4, R) + 16 * j);
         const uint32_t RF = lds_u16(base + col_offset<L>(5, R) + 2 * j);
         const uint32_t LS = lds_u16(base + col_offset<L>(6, R) + 2 * j);
+        // Both rows in the fast domain (always, in TPC-H data): the placement's tables only. A
+        // per-thread branch, not a warp vote: the warp-lane placement's lanes may diverge here.
+        const bool fast = ((Q.y | Q.w | D.y | D.w | X.y | X.w | P.y | P.w) == 0u) & (D.x <= 100u) & (D.z <= 100u) &
+                          (X.x <= 255u) & (X.z <= 255u);
+        if (fast) {
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int32_t ship = (int32_t)(r ? sd.y : sd.x);
-            const uint32_t code = code_of_chars((RF >> (8 * r)) & 0xFFu, (LS >> (8 * r)) & 0xFFu);
-            const uint32_t q = r ? Q.z : Q.x;
-            const uint32_t d = r ? D.z : D.x;
-            const uint32_t t = r ? X.z : X.x;
-            const uint32_t p = r ? P.z : P.x;
-            const bool wide = ((r ? (Q.w | D.w | X.w | P.w) : (Q.y | D.y | X.y | P.y)) != 0u) | (d > 100u) | (t > 255u);
-            const bool pass = ship <= cut;
-            if (wide && pass && acc.owns(code))
-                wide_row(prm, code, (int64_t)((uint64_t)(r ? Q.w : Q.y) << 32 | q),
-                         (int64_t)((uint64_t)(r ? D.w : D.y) << 32 | d), (int64_t)((uint64_t)(r ? X.w : X.y) << 32 | t),
-                         (int64_t)((uint64_t)(r ? P.w : P.y) << 32 | p));
-            const uint32_t c = (pass && !wide) ? code : 7u;
-            const uint32_t a = 100u - d;
-            acc.add(c, q, d, a, a * (100u + t), p);
+            for (int r = 0; r < 2; ++r) {
+                const int32_t ship = (int32_t)(r ? sd.y : sd.x);
+                const uint32_t code = code_of_chars((RF >> (8 * r)) & 0xFFu, (LS >> (8 * r)) & 0xFFu);
+                const uint32_t c = ship <= cut ? code : 7u;
+                const uint32_t q = r ? Q.z : Q.x;
+                const uint32_t d = r ? D.z : D.x;
+                const uint32_t t = r ? X.z : X.x;
+                const uint32_t p = r ? P.z : P.x;
+                const uint32_t a = 100u - d;
+                acc.add(c, q, d, a, a * (100u + t), p);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int32_t ship = (int32_t)(r ? sd.y : sd.x);
+                const uint32_t code = code_of_chars((RF >> (8 * r)) & 0xFFu, (LS >> (8 * r)) & 0xFFu);
+                const uint32_t q = r ? Q.z : Q.x;
+                const uint32_t d = r ? D.z : D.x;
+                const uint32_t t = r ? X.z : X.x;
+                const uint32_t p = r ? P.z : P.x;
+                const bool wide =
+                    ((r ? (Q.w | D.w | X.w | P.w) : (Q.y | D.y | X.y | P.y)) != 0u) | (d > 100u) | (t > 255u);
+                const bool pass = ship <= cut;
+                if (wide && pass && acc.owns(code))
+                    wide_row(prm, code, (int64_t)((uint64_t)(r ? Q.w : Q.y) << 32 | q),
+                             (int64_t)((uint64_t)(r ? D.w : D.y) << 32 | d),
+                             (int64_t)((uint64_t)(r ? X.w : X.y) << 32 | t),
+                             (int64_t)((uint64_t)(r ? P.w : P.y) << 32 | p));
+                const uint32_t c = (pass && !wide) ? code : 7u;
+                const uint32_t a = 100u - d;
+                acc.add(c, q, d, a, a * (100u + t), p);
+            }
         }
     } else {
         constexpr bool kSep = (L == kLaySep || L == kLaySepFilter);
