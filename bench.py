@@ -500,6 +500,20 @@ def main():
     return 0
 
 
+def event_timed(call):
+    """Seconds one synchronous public-API call takes, from CUDA events recorded on the current
+    stream right before and right after it (the call returns once its copies, kernels and host
+    work are done, so the events bracket all of it)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    call()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / 1e3
+
+
 def e2e_sharded(q, args, rank, world, local_rank, dist):
     """e2e at N > 1 GPUs (weak scaling): every rank streams its own 600 M-row shard from pinned host
     memory through q1_run over its own PCIe link (GPU only: filter pushdown and coprocessing would
@@ -516,10 +530,7 @@ def e2e_sharded(q, args, rank, world, local_rank, dist):
         ctx.run(p)
         steps = max(3, min(args.steps, 10))
         dist.barrier()
-        s = time.perf_counter()
-        for _ in range(steps):
-            ctx.run(p)
-        el = torch.tensor([time.perf_counter() - s], device="cuda")
+        el = torch.tensor([sum(event_timed(lambda: ctx.run(p)) for _ in range(steps))], device="cuda")
         dist.all_reduce(el, op=dist.ReduceOp.MAX)
         t = float(el.item())
         h2d = int(rows * 9 + 4 * ((rows + 15) // 16)) * world
@@ -547,12 +558,7 @@ def e2e_pinned(q, args):
                               num_tuples_per_kernel_launch=1 << 24, num_query_execution_runs=1, cutoff_day=CUTOFF)
 
         def timed(p, n):
-            t = []
-            for _ in range(n):
-                s = time.perf_counter()
-                ctx.run(p)
-                t.append(time.perf_counter() - s)
-            return t
+            return [event_timed(lambda: ctx.run(p)) for _ in range(n)]
 
         sweep = {}
         frac, worse = 0.25, 0
@@ -818,12 +824,7 @@ def bench_c1sweep(args):
                            cpu_processing_fraction=frac, num_gpu_streams=4, num_tuples_per_kernel_launch=1 << 24,
                            num_query_execution_runs=1, cutoff_day=CUTOFF)
             ctx.run(p)
-            t = []
-            for _ in range(3):
-                s0 = time.perf_counter()
-                ctx.run(p)
-                t.append(time.perf_counter() - s0)
-            ms = 1000 * min(t)
+            ms = 1000 * min(event_timed(lambda: ctx.run(p)) for _ in range(3))
             gpu_b = ROWS * (1 - frac) * (7.375 if pushdown else 9.25)
             streamed.append({"pushdown": pushdown, "cpu_fraction": frac, "ms": ms, "rows_per_s": ROWS / (ms / 1e3),
                              "pcie_gbs": gpu_b / (ms / 1e3) / 1e9})

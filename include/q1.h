@@ -642,8 +642,9 @@ q1_status q1_server_close(q1_server* server);
 typedef enum q1_fault {
     Q1_FAULT_NONE         = 0,   /* clears every pending fault */
     Q1_FAULT_CPU_WORKER   = 1,   /* the next CPU pool jobs raise (Q1_ERR_CPU_WORKER from q1_run) */
-    Q1_FAULT_DEVICE_ALLOC = 2,   /* the next context device allocations fail (Q1_ERR_OUT_OF_MEMORY) */
-    Q1_FAULT_PINNED_ALLOC = 3,   /* the next context pinned host allocations fail */
+    Q1_FAULT_DEVICE_ALLOC = 2,   /* the next context, .tbl reader and server device allocations fail
+                                    (Q1_ERR_OUT_OF_MEMORY) */
+    Q1_FAULT_PINNED_ALLOC = 3,   /* the next context, .tbl reader and server pinned host allocations fail */
     Q1_FAULT_SERVE_ROUND  = 4    /* the next serving rounds fail to enqueue (Q1_ERR_INTERNAL): the
                                     server fails that round, the rounds behind it and every queued
                                     request, and refuses later submissions */

@@ -122,3 +122,27 @@ def test_failed_serving_round_fails_what_follows_and_server_reopens(cuda):
         assert np.array_equal(words(resp), words(ok))
     finally:
         _lib.check(L.q1_server_close(h2))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", [2, 3])
+def test_server_open_fails_cleanly_and_reopens(cuda, kind):
+    """An allocation that fails while q1_server_open builds its state is reported as
+    Q1_ERR_OUT_OF_MEMORY with no server made, what was built is released, and the next open on the
+    same device answers exactly. The first device allocation (the resident table) fails after the
+    streams exist; the first pinned one (a round lane's buffers) after the resident table, its
+    per-day cubes and the ad-hoc arena are built."""
+    from test_gpu_serve import FLAGS, KEYS, RES, open_server, plain, req, submit, wait, words
+    L = q.lib()
+    free0 = torch.cuda.mem_get_info()[0]
+    _lib.check(L.q1_inject_fault(kind, 1))
+    with pytest.raises(q.Q1Error) as e:
+        open_server()
+    assert e.value.status == 3 and "injected" in str(e.value)
+    assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)   # the partial build was released
+    h = open_server()
+    try:
+        for r in (req(RES, FLAGS, 729999), req(RES, KEYS, 728826, 64)):
+            assert np.array_equal(words(wait(h, submit(h, r))), words(plain(h, r)))
+    finally:
+        _lib.check(L.q1_server_close(h))

@@ -78,6 +78,7 @@ struct Dev {
     }
     q1_status alloc(uint64_t bytes) {
         release();
+        if (take_fault(kFaultDeviceAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected device allocation failure");
         cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -102,6 +103,7 @@ struct Pinned {
     }
     q1_status alloc(uint64_t bytes) {
         release();
+        if (take_fault(kFaultPinnedAlloc)) return set_error(Q1_ERR_OUT_OF_MEMORY, "injected pinned allocation failure");
         cudaError_t e = cudaHostAlloc(&p, bytes ? bytes : 16, cudaHostAllocDefault);
         if (e != cudaSuccess) {
             p = nullptr;
@@ -778,6 +780,33 @@ void q1_server_opts_default(q1_server_opts* o) {
     o->max_adhoc_rows = 100000000ull;
 }
 
+namespace {
+
+// Device state of a server whose options are valid: streams, resident table and cubes, arena,
+// lanes. On failure the caller closes the server, which releases whatever was made.
+q1_status server_setup(q1_server* s) {
+    s->device = s->opts.device;
+    Q1_CUDA(cudaSetDevice(s->device));
+    q1_status st = device_info(s->device, &s->di);
+    if (st != Q1_OK) return st;
+    Q1_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    Q1_CUDA(cudaStreamCreateWithFlags(&s->plain_stream, cudaStreamNonBlocking));
+    Q1_CUDA(batch_prepare_launch());
+    s->res_rows = s->opts.resident_rows;
+    if ((st = build_resident(s)) != Q1_OK) return st;
+    if ((st = s->arena_mem.alloc(s->opts.hbm_budget_bytes)) != Q1_OK) return st;
+    s->arena.reset(s->opts.hbm_budget_bytes);
+    const uint32_t nlanes = s->opts.mode == Q1_SERVE_PLAIN ? 1u : s->opts.max_rounds_in_flight;
+    for (uint32_t i = 0; i < nlanes; ++i) {
+        s->lanes.emplace_back(new Lane());
+        if ((st = lane_open(s->lanes.back().get(), s->opts.max_inflight)) != Q1_OK) return st;
+        s->free_lanes.push_back(s->lanes.back().get());
+    }
+    return s->plain_scratch.alloc(q1_groupkey_scratch_bytes(kMaxGroups));
+}
+
+}  // namespace
+
 q1_status q1_server_open(const q1_server_opts* opts, q1_server** out) {
     if (!out) return set_error(Q1_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
@@ -792,24 +821,12 @@ q1_status q1_server_open(const q1_server_opts* opts, q1_server** out) {
     if (s->opts.resident_rows > (1ull << 40)) return set_error(Q1_ERR_INVALID_ARGUMENT, "resident table too large");
     if (s->opts.max_adhoc_rows > (uint64_t)UINT32_MAX * kBatchTileRows)
         return set_error(Q1_ERR_INVALID_ARGUMENT, "max_adhoc_rows too large");
-    s->device = s->opts.device;
-    Q1_CUDA(cudaSetDevice(s->device));
-    q1_status st = device_info(s->device, &s->di);
-    if (st != Q1_OK) return st;
-    Q1_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    Q1_CUDA(cudaStreamCreateWithFlags(&s->plain_stream, cudaStreamNonBlocking));
-    Q1_CUDA(batch_prepare_launch());
-    s->res_rows = s->opts.resident_rows;
-    if ((st = build_resident(s.get())) != Q1_OK) return st;
-    if ((st = s->arena_mem.alloc(s->opts.hbm_budget_bytes)) != Q1_OK) return st;
-    s->arena.reset(s->opts.hbm_budget_bytes);
-    const uint32_t nlanes = s->opts.mode == Q1_SERVE_PLAIN ? 1u : s->opts.max_rounds_in_flight;
-    for (uint32_t i = 0; i < nlanes; ++i) {
-        s->lanes.emplace_back(new Lane());
-        if ((st = lane_open(s->lanes.back().get(), s->opts.max_inflight)) != Q1_OK) return st;
-        s->free_lanes.push_back(s->lanes.back().get());
+    const q1_status st = server_setup(s.get());
+    if (st != Q1_OK) {
+        const std::string msg = q1_last_error();
+        q1_server_close(s.release());   // streams, events and lanes made so far
+        return set_error(st, msg);
     }
-    if ((st = s->plain_scratch.alloc(q1_groupkey_scratch_bytes(kMaxGroups))) != Q1_OK) return st;
     s->completer = std::thread(completer_loop, s.get());
     s->dispatcher = std::thread(dispatcher_loop, s.get());
     *out = s.release();
