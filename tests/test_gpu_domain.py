@@ -8,10 +8,13 @@ wide tax / discount / quantity bytes run under test in every placement, both fla
 with filter pushdown off and on, plus the uncompressed (reference-typed) layout.
 
 The exactness bound of the per-thread 32-bit partials (2^15 rows per consumer thread per launch,
-which the host enforces by splitting launches) is pinned with a one-CTA launch over maximal
-bytes: 2^23 rows give every one of its 256 consumer threads exactly 2^15 rows in the first
-launch, then a second launch takes the ragged rest. A group's sum_charge there passes 2^64, so
-the 128-bit carries of the warp, CTA and global reductions run too."""
+which the host enforces by splitting launches at whole tiles) is pinned with one-CTA launches over
+maximal bytes: 384 x 2^15 + 4099 rows give each consumer thread of the CTA (256, 320 or 384 of
+them, by layout and placement) 2^15 rows in its first launch where the tile is 4096 rows, and
+32,760 (the last whole tile below the bound) where it is 3840 or 4608 rows; further launches take
+the ragged rest. A group's
+sum_charge there passes 2^64, so the 128-bit carries of the warp, CTA and global reductions run
+too."""
 import numpy as np
 import pytest
 import torch
@@ -109,7 +112,7 @@ def maximal_rows(rows, seed):
 
 @pytest.fixture(scope="module")
 def maximal():
-    rows = (1 << 23) + 4099
+    rows = 384 * (1 << 15) + 4099
     cols = maximal_rows(rows, 7)
     return cols, oracle_table(cols)
 

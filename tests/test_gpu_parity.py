@@ -97,8 +97,10 @@ def test_pinned_filter_pushdown_with_cpu_producers(cuda, cols, packing, coproc):
         assert np.array_equal(res.table(), oracle(cols))
 
 
-@pytest.mark.parametrize("rows", [0, 1, 31, 32, 33, 127, 128, 4095, 4096, 4097, 8197, 1_000_003])
+@pytest.mark.parametrize("rows", [0, 1, 31, 32, 33, 127, 128, 4095, 4096, 4097, 4607, 4608, 4609, 8197, 9217,
+                                  1_000_003])
 @pytest.mark.parametrize("kind", [("compressed", "pair", "in_registers_per_thread"),
+                                  ("compressed", "pair", "shared_mem_per_thread"),
                                   ("uncompressed", "pair", "in_registers"),
                                   ("compressed", "separate", "global")])
 def test_ragged_and_tiny_tables(cuda, rows, kind):

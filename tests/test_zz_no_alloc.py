@@ -71,11 +71,12 @@ def test_noalloc_matches_allocating_entry_point_twice(placement, packing, use_fi
         assert int(want[:, 0].sum()) > 0
 
 
-@pytest.mark.parametrize("placement,rows", [("in_registers", 4_500_001), ("in_registers_per_thread", 8_400_007)])
+@pytest.mark.parametrize("placement,rows", [("in_registers", 4_500_001), ("in_registers_per_thread", 12_600_007)])
 def test_noalloc_one_cta_several_chunks(placement, rows):
-    """One CTA: the host splits the rows into launches of at most 2^15 rows per accumulating lane
-    (2,097,152 rows for in_registers' 64 lanes, 8,388,608 for in_registers_per_thread's 256), and
-    every launch reuses the same record, then two such calls in a row."""
+    """One CTA: the host splits the rows into launches of whole tiles and at most 2^15 rows per
+    accumulating lane (pair layout, 12 consumer warps, 4608-row tiles: 3,142,656 rows for
+    in_registers' 96 lanes, 12,579,840 for in_registers_per_thread's 384), and every launch reuses
+    the same record, then two such calls in a row."""
     L = q.lib()
     stream = torch.cuda.current_stream().cuda_stream
     for seed, n in [(902, rows), (903, rows // 3)]:

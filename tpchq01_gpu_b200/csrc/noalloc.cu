@@ -166,7 +166,7 @@ extern "C" q1_status q1_launch_compressed_noalloc(q1_placement placement, const 
             max_blocks = (int)std::min<uint64_t>((rows + per - 1) / per, (uint64_t)sms);
         }
     }
-    const uint32_t grid = scan_grid_blocks(layout, rows, sms, max_blocks);
+    const uint32_t grid = scan_grid_blocks(layout, placement, rows, sms, max_blocks);
     const uint64_t kMaxRows = scan_max_rows_per_launch(layout, placement, grid);
     if (grid > kNoAllocMaxCtas)
         return set_error(Q1_ERR_INVALID_ARGUMENT,
@@ -196,7 +196,7 @@ extern "C" q1_status q1_launch_compressed_noalloc(q1_placement placement, const 
         prm.out = reinterpret_cast<unsigned long long*>(dev_aggregates);
         prm.status = status;
         prm.records = records;
-        const uint32_t nrec = scan_grid_blocks(layout, n, sms, max_blocks);
+        const uint32_t nrec = scan_grid_blocks(layout, placement, n, sms, max_blocks);
         cudaError_t e = launch_scan(layout, placement, prm, sms, max_blocks, stream);
         if (e != cudaSuccess) return cuda_error(e, "scan kernel launch");
         noalloc_reduce_records<<<1, 64, 0, stream>>>(records, nrec, reinterpret_cast<unsigned long long*>(dev_aggregates));

@@ -714,7 +714,7 @@ static q1_status run_once(q1_ctx* ctx, const q1_params* prm, Agg128* total, doub
     uint64_t cpu_start = N;
     if (coproc) {
         cpu_start = N - (uint64_t)((double)N * prm->cpu_fraction);
-        const uint64_t unit = streamed ? (uint64_t)prm->tuples_per_launch : (uint64_t)scan_tile_rows(kLayPair);
+        const uint64_t unit = streamed ? (uint64_t)prm->tuples_per_launch : (uint64_t)scan_tile_rows(kLayPair, kPlaceInRegistersPerThread);
         cpu_start -= cpu_start % unit;
     }
     const uint64_t gpu_end = cpu_start;

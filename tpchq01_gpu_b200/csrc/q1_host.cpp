@@ -400,7 +400,7 @@ static q1_status scan_launch(int layout, q1_placement placement, const uint8_t* 
 
     // Launch size bound that keeps every per-thread partial exact (scan_max_rows_per_launch).
     const uint64_t kMaxRows =
-        scan_max_rows_per_launch(layout, placement, scan_grid_blocks(layout, rows, di->sm_count, max_blocks));
+        scan_max_rows_per_launch(layout, placement, scan_grid_blocks(layout, placement, rows, di->sm_count, max_blocks));
     for (uint64_t off = 0; off < rows; off += kMaxRows) {
         const uint64_t n = std::min(kMaxRows, rows - off);
         ScanParams prm{};

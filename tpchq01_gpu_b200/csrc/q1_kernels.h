@@ -25,24 +25,35 @@ enum ScanPlacement : int {
     kPlaceGlobal = 4,
 };
 
-// Rows per tile (one bulk copy per column per tile); a multiple of 128 so that every column
-// slice of every tile starts on a 16-byte boundary, down to 1-bit columns.
-template <int L>
-inline constexpr uint32_t kTileRows = (L == kLayUncomp) ? 1024u : 4096u;
+// Consumer warps per CTA (plus one producer warp), per input layout and placement, as measured on
+// the 600 M-row table (100 M uncompressed). More warps per SM sub-partition hide more of the decode's
+// issue latency where the registers allow: the pair layouts' kernels fit the 128 registers a thread
+// that 13 warps leave and run 12 (in_registers_per_thread 0.909 -> 0.871 ms, in_registers, shared and
+// global 5-20% faster); the separate-flag and uncompressed layouts need up to 168 and run 10
+// (separate per-thread 1.129 -> 1.041 ms, shared 3.04 -> 2.71, global 1.31 -> 1.21; uncompressed
+// per-thread 0.625 -> 0.600 although one of its registers spills, shared 0.670 -> 0.548). local_mem keeps 8 with compressed rows (its
+// per-thread tables run out of L1 with more threads: pair 2.83 -> 3.06 ms), and so does the
+// separate layout's in_registers (3.58 -> 3.65 ms with 10).
+template <int L, int P>
+inline constexpr uint32_t kConsumerWarps =
+    (L == kLayPair || L == kLayPairFilter) ? (P == kPlaceLocalMem ? 8u : 12u)
+    : (L == kLaySep || L == kLaySepFilter) ? ((P == kPlaceLocalMem || P == kPlaceInRegisters) ? 8u : 10u)
+                                           : 10u;
+// Rows per tile (one bulk copy per column per tile): a multiple of 128, so that every column slice
+// of every tile starts on a 16-byte boundary down to 1-bit columns, and of the consumer threads x
+// the rows of a step, so that a tile's steps divide evenly among the consumer threads.
+template <int L, int P>
+inline constexpr uint32_t kTileRows =
+    (L == kLayUncomp) ? 128u * kConsumerWarps<L, P> : (kConsumerWarps<L, P> == 8u ? 4096u : 384u * kConsumerWarps<L, P>);
 // Shared-memory ring depth.
 template <int L, int P>
 inline constexpr uint32_t kStages = (P == kPlaceSharedMemPerThread) ? 3u : 4u;
-// Consumer warps per CTA (plus one producer warp).
-#ifndef Q1_CONSUMER_WARPS
-#define Q1_CONSUMER_WARPS 8
-#endif
-inline constexpr uint32_t kConsumerWarps = Q1_CONSUMER_WARPS;
 // Tiles a warp of the global placement write-combines in registers between its atomic adds into
-// the global table (each warp adds 16 rows per thread of a 4096-row tile, so 65,536 rows per warp
-// between flushes; about 8 flushes per warp over 600 M rows). Measured on 600 M rows: 1 tile
-// 12.94 ms (same-address L2 atomics serialise: 7.1 M atomic requests per 100 M rows), 4 tiles
-// 4.05 ms, 16 tiles 1.95 ms, 64 tiles 1.22 ms, 128 tiles 1.08 ms. 128 is the most a 64-bit warp
-// sum allows (AccGlobal's static_assert).
+// the global table (12 or 16 rows per thread of a compressed tile, so 49,152 or 65,536 rows per warp
+// between flushes; a few flushes per warp over 600 M rows). Measured on 600 M rows (8 warps,
+// 4096-row tiles): 1 tile 12.94 ms (same-address L2 atomics serialise: 7.1 M atomic requests per
+// 100 M rows), 4 tiles 4.05 ms, 16 tiles 1.95 ms, 64 tiles 1.22 ms, 128 tiles 1.08 ms. A 64-bit
+// warp sum bounds the rows a thread may buffer (the kernel's static_assert).
 #ifndef Q1_GLOBAL_FLUSH_TILES
 #define Q1_GLOBAL_FLUSH_TILES 128
 #endif
@@ -64,9 +75,10 @@ struct ScanParams {
 // Launch the scan kernel for one layout x placement. max_blocks <= 0: one CTA per SM.
 cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm_count, int max_blocks,
                         cudaStream_t stream);
-uint32_t scan_tile_rows(int layout);
-// Grid size launch_scan uses for `rows` rows of `layout`.
-uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks);
+// Rows per tile of the layout x placement (a multiple of 128).
+uint32_t scan_tile_rows(int layout, int placement);
+// Grid size launch_scan uses for `rows` rows of the layout x placement.
+uint32_t scan_grid_blocks(int layout, int placement, uint64_t rows, int sm_count, int max_blocks);
 // Most rows one launch may take so that no consumer thread adds more than 2^15 rows (which keeps
 // its 32-bit and 64-bit partial sums exact) and per-launch sums stay below 2^31 rows.
 uint64_t scan_max_rows_per_launch(int layout, int placement, uint32_t grid);

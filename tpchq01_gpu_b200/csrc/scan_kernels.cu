@@ -521,9 +521,9 @@ struct AccSharedPerThread {
 // (group, aggregate) straight into the global table and empties the buffer.
 template <int G, bool kWideQty>
 struct AccGlobal {
-    // A warp's flush of one sum is a 64-bit warp reduction: at most 32 lanes x 16 rows x 128
-    // tiles of charges below 100 (2^32 - 1) 355 < 2^47.2 stays below 2^64.
-    static_assert(kGlobalFlushTiles >= 1 && kGlobalFlushTiles <= 128, "flush sums must stay below 2^64");
+    // A warp's flush of one sum is a 64-bit warp reduction; the kernel bounds the rows a lane
+    // buffers between flushes so that it cannot wrap.
+    static_assert(kGlobalFlushTiles >= 1, "flush cadence");
     AccPerThread<G, kWideQty> buf;
     uint32_t tiles;
     __device__ __forceinline__ void init(uint32_t a, uint32_t b, uint8_t* s) {
@@ -613,12 +613,11 @@ __device__ __noinline__ void wide_row(const ScanParams& prm, uint32_t group, int
     atomic_add_i128(o + 2 * kAggCharge, ch);
 }
 
-// One step of rows [kRowsPerStep * j, +kRowsPerStep) of the tile held at shared address `base`.
-template <int L, class Acc>
+// One step of rows [kRowsPerStep * j, +kRowsPerStep) of the R-row tile held at shared address `base`.
+template <int L, uint32_t R, class Acc>
 __device__ __forceinline__ void process_step(const ScanParams& prm, uint32_t base, uint32_t j, int32_t cut,
                                              uint32_t lut, Acc& acc, uint32_t& bad) {
     using T = LayoutTraits<L>;
-    constexpr uint32_t R = kTileRows<L>;
     if constexpr (L == kLayUncomp) {
         const uint2 sd = lds_v2(base + col_offset<L>(0, R) + 8 * j);
         const uint4 Q = lds_v4(base + col_offset<L>(1, R) + 16 * j);
@@ -753,12 +752,12 @@ __device__ __forceinline__ void process_row_global(const ScanParams& prm, uint64
 // ---------------------------------------------------------------------------------------------
 
 template <int L, int P>
-__global__ void __launch_bounds__((kConsumerWarps + 1) * 32, 1)
+__global__ void __launch_bounds__((kConsumerWarps<L, P> + 1) * 32, 1)
 q1_scan_kernel(const __grid_constant__ ScanParams prm) {
     using T = LayoutTraits<L>;
-    constexpr uint32_t R = kTileRows<L>;
+    constexpr uint32_t R = kTileRows<L, P>;
     constexpr uint32_t S = kStages<L, P>;
-    constexpr uint32_t W = kConsumerWarps;
+    constexpr uint32_t W = kConsumerWarps<L, P>;
     constexpr uint32_t kStage = stage_bytes<L>(R);
     constexpr int G = T::kCodes;
     static_assert(kStage % 16 == 0, "stage must keep 16-byte alignment");
@@ -831,6 +830,10 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
         constexpr uint32_t kFoldEvery = (257u / kRowsPerThreadTile) > 0 ? (257u / kRowsPerThreadTile) : 1u;
         static_assert(kRowsPerThreadTile <= 257u, "tile too large for the packed partials");
         static_assert(kSteps % (W * 32) == 0, "steps must divide evenly among consumer threads");
+        // The global placement's warp flush is a 64-bit sum of 32 lanes' buffered rows: at most
+        // 2048 rows a lane of charges below 100 (2^32 - 1) 355 < 2^47.2 stays below 2^64.
+        static_assert(P != kPlaceGlobal || kRowsPerThreadTile * kGlobalFlushTiles <= 2048u,
+                      "global flush sums must stay below 2^64");
         bool ok = true;
         uint32_t k = 0;
         for (uint64_t t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {
@@ -846,12 +849,12 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
                 const uint32_t tbl = lane / G;
                 if (tbl < kTablesPerWarp) {
                     for (uint32_t j = warp * kTablesPerWarp + tbl; j < kSteps; j += W * kTablesPerWarp)
-                        process_step<L>(prm, base, j, prm.cutoff, lut, acc, bad);
+                        process_step<L, R>(prm, base, j, prm.cutoff, lut, acc, bad);
                 }
             } else {
 #pragma unroll
                 for (uint32_t it = 0; it < kSteps / (W * 32); ++it)
-                    process_step<L>(prm, base, ctid + it * (W * 32), prm.cutoff, lut, acc, bad);
+                    process_step<L, R>(prm, base, ctid + it * (W * 32), prm.cutoff, lut, acc, bad);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
@@ -924,15 +927,15 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
 
 template <int L, int P>
 static cudaError_t launch_one(const ScanParams& prm, int sm_count, int max_blocks, cudaStream_t stream) {
-    constexpr uint32_t R = kTileRows<L>;
+    constexpr uint32_t R = kTileRows<L, P>;
     constexpr uint32_t S = kStages<L, P>;
-    constexpr uint32_t W = kConsumerWarps;
+    constexpr uint32_t W = kConsumerWarps<L, P>;
     constexpr int G = LayoutTraits<L>::kCodes;
     uint32_t dyn = S * stage_bytes<L>(R);
     if (P == kPlaceSharedMemPerThread) dyn += (uint32_t)(8 * (L == kLayUncomp ? 5 : 4) * G * W * 32);
     cudaError_t e = cudaFuncSetAttribute(q1_scan_kernel<L, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
-    const uint32_t blocks = scan_grid_blocks(L, prm.rows, sm_count, max_blocks);
+    const uint32_t blocks = scan_grid_blocks(L, P, prm.rows, sm_count, max_blocks);
     q1_scan_kernel<L, P><<<blocks, (W + 1) * 32, dyn, stream>>>(prm);
     return cudaGetLastError();
 }
@@ -961,18 +964,47 @@ cudaError_t launch_scan(int layout, int placement, const ScanParams& prm, int sm
     }
 }
 
+namespace {
+
+struct Geometry {
+    uint32_t warps, tile_rows;
+};
+template <int L>
+Geometry geometry_of(int placement) {
+    switch (placement) {
+        case kPlaceInRegisters: return {kConsumerWarps<L, kPlaceInRegisters>, kTileRows<L, kPlaceInRegisters>};
+        case kPlaceInRegistersPerThread:
+            return {kConsumerWarps<L, kPlaceInRegistersPerThread>, kTileRows<L, kPlaceInRegistersPerThread>};
+        case kPlaceLocalMem: return {kConsumerWarps<L, kPlaceLocalMem>, kTileRows<L, kPlaceLocalMem>};
+        case kPlaceSharedMemPerThread:
+            return {kConsumerWarps<L, kPlaceSharedMemPerThread>, kTileRows<L, kPlaceSharedMemPerThread>};
+        default: return {kConsumerWarps<L, kPlaceGlobal>, kTileRows<L, kPlaceGlobal>};
+    }
+}
+Geometry geometry(int layout, int placement) {
+    switch (layout) {
+        case kLayPair: return geometry_of<kLayPair>(placement);
+        case kLayPairFilter: return geometry_of<kLayPairFilter>(placement);
+        case kLaySep: return geometry_of<kLaySep>(placement);
+        case kLaySepFilter: return geometry_of<kLaySepFilter>(placement);
+        default: return geometry_of<kLayUncomp>(placement);
+    }
+}
+
+}  // namespace
+
 uint64_t scan_max_rows_per_launch(int layout, int placement, uint32_t grid) {
     // accumulating lanes per CTA: every consumer thread, or the lanes of one warp-lane table
     const uint64_t codes = (layout == kLayPair || layout == kLayPairFilter) ? 4 : 6;
-    const uint64_t lanes = placement == kPlaceInRegisters ? kConsumerWarps * (32 / codes) : kConsumerWarps * 32;
+    const Geometry g = geometry(layout, placement);
+    const uint64_t lanes = placement == kPlaceInRegisters ? g.warps * (32 / codes) : g.warps * 32ull;
     uint64_t n = (uint64_t)grid * lanes * 32768ull;
     if (n > (1ull << 31)) n = 1ull << 31;
-    const uint64_t tile = scan_tile_rows(layout);
-    return n / tile * tile;
+    return n / g.tile_rows * g.tile_rows;
 }
 
-uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_blocks) {
-    const uint64_t tiles = rows / scan_tile_rows(layout);
+uint32_t scan_grid_blocks(int layout, int placement, uint64_t rows, int sm_count, int max_blocks) {
+    const uint64_t tiles = rows / scan_tile_rows(layout, placement);
     uint64_t blocks = tiles ? tiles : 1;
     uint64_t cap = (uint64_t)sm_count;  // one CTA per SM (shared-memory bound)
     if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
@@ -980,11 +1012,6 @@ uint32_t scan_grid_blocks(int layout, uint64_t rows, int sm_count, int max_block
     return (uint32_t)blocks;
 }
 
-uint32_t scan_tile_rows(int layout) {
-    switch (layout) {
-        case kLayUncomp: return kTileRows<kLayUncomp>;
-        default: return kTileRows<kLayPair>;
-    }
-}
+uint32_t scan_tile_rows(int layout, int placement) { return geometry(layout, placement).tile_rows; }
 
 }  // namespace q1
