@@ -65,11 +65,24 @@ def test_launch_compressed(cuda, placement, packing, use_filter):
 @pytest.mark.parametrize("placement", PLACEMENTS)
 @pytest.mark.parametrize("packing", ["pair", "sep"])
 @pytest.mark.parametrize("frac", [0.0005, 0.3])
-def test_all_six_flag_groups(cuda, placement, packing, frac):
+@pytest.mark.parametrize("use_filter,wide", [(False, False), (True, False), (False, True)])
+def test_all_six_flag_groups(cuda, placement, packing, frac, use_filter, wide):
     """Rows of the groups A/O and R/O (absent from TPC-H data) change some rows' line status to O:
-    every placement must still sum all six (returnflag, linestatus) groups exactly."""
+    every placement must still sum all six (returnflag, linestatus) groups exactly, with filter
+    pushdown too, and with a tenth of the rows carrying bytes from the whole compressed domain
+    (prices up to 2^32 - 1, tax up to 255, discount up to 100, quantity up to 255)."""
     cols = gen_np.generate(32, 0, 200_003)
     rng = np.random.default_rng(int(frac * 1e4))
+    if wide:
+        n = len(cols["shipdate"])
+        idx = rng.choice(n, n // 10, replace=False)
+        cols["extendedprice"] = cols["extendedprice"].copy()
+        cols["extendedprice"][idx] = rng.integers(1 << 24, 1 << 32, len(idx))
+        for k, hi in [("tax", 256), ("discount", 101)]:
+            cols[k] = cols[k].copy()
+            cols[k][idx] = rng.integers(0, hi, len(idx))
+        cols["quantity"] = cols["quantity"].copy()
+        cols["quantity"][idx] = rng.integers(0, 256, len(idx)) * 100
     rf = cols["returnflag"].view(np.uint8)
     ls = cols["linestatus"].view(np.uint8).copy()
     idx = np.flatnonzero(rf != ord("N"))
@@ -82,10 +95,12 @@ def test_all_six_flag_groups(cuda, placement, packing, frac):
         cols = {k: v[keep] for k, v in cols.items()}
     comp = gen_np.compress(cols, packing)
     cutoff = 729999
+    if use_filter:
+        comp["filter"] = gen_np.filter_bitmap(comp["shipdate"], cutoff)
     c, keep_ = device_compressed(comp)
     buf = aggs_buffer()
     stream = torch.cuda.current_stream().cuda_stream
-    q.launch_compressed(placement, c, len(cols["shipdate"]), cutoff, False, buf.data_ptr(), stream)
+    q.launch_compressed(placement, c, len(cols["shipdate"]), cutoff, use_filter, buf.data_ptr(), stream)
     q.sync_check(stream)
     want, flag = O.q1_compressed(comp, cutoff)
     assert flag == 0

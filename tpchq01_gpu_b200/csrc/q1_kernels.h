@@ -27,18 +27,23 @@ enum ScanPlacement : int {
 
 // Consumer warps per CTA (plus one producer warp), per input layout and placement, as measured on
 // the 600 M-row table (100 M uncompressed). More warps per SM sub-partition hide more of the decode's
-// issue latency where the registers allow: the pair layouts' kernels fit the 128 registers a thread
-// that 13 warps leave and run 12 (in_registers_per_thread 0.909 -> 0.871 ms, in_registers, shared and
-// global 5-20% faster); the separate-flag and uncompressed layouts need up to 168 and run 10
-// (separate per-thread 1.129 -> 1.041 ms, shared 3.04 -> 2.71, global 1.31 -> 1.21; uncompressed
-// per-thread 0.625 -> 0.600 although one of its registers spills, shared 0.670 -> 0.548). local_mem keeps 8 with compressed rows (its
-// per-thread tables run out of L1 with more threads: pair 2.83 -> 3.06 ms), and so does the
+// issue latency where the registers allow. 12 warps leave 128 registers a thread (13 warps, which the
+// allocator rounds up to 16 warps' worth): the pair layouts' kernels fit (in_registers_per_thread
+// 0.909 -> 0.871 ms; in_registers, shared and global 5-20% faster), and so do the separate-flag
+// layouts' register placements, which keep only four groups' planes in registers (A/O and R/O go
+// to the CTA's shared table: per-thread 1.129 ms with 8 warps and six planes, 1.044 with 10, 0.980
+// with 12; global 1.31 -> 1.22 -> 1.16). Their shared placement runs 10 (3.04 -> 2.71 ms), and so
+// does the uncompressed layout, which needs up to 168 registers (per-thread 0.625 -> 0.600 ms
+// although one register spills; shared 0.670 -> 0.548). local_mem keeps 8 with compressed rows
+// (its per-thread tables run out of L1 with more threads: pair 2.83 -> 3.06 ms), and so does the
 // separate layout's in_registers (3.58 -> 3.65 ms with 10).
 template <int L, int P>
 inline constexpr uint32_t kConsumerWarps =
     (L == kLayPair || L == kLayPairFilter) ? (P == kPlaceLocalMem ? 8u : 12u)
-    : (L == kLaySep || L == kLaySepFilter) ? ((P == kPlaceLocalMem || P == kPlaceInRegisters) ? 8u : 10u)
-                                           : 10u;
+    : (L == kLaySep || L == kLaySepFilter)
+        ? ((P == kPlaceLocalMem || P == kPlaceInRegisters) ? 8u
+                                                           : ((P == kPlaceSharedMemPerThread) ? 10u : 12u))
+        : 10u;
 // Rows per tile (one bulk copy per column per tile): a multiple of 128, so that every column slice
 // of every tile starts on a 16-byte boundary down to 1-bit columns, and of the consumer threads x
 // the rows of a step, so that a tile's steps divide evenly among the consumer threads.

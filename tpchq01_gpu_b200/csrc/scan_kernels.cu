@@ -218,19 +218,47 @@ struct CtaRed {
 // (src/kernels/ht_in_registers_per_thread.cuh:11-79).
 template <int G, bool kWideQty>
 struct AccPerThread {
+    // With the six (returnflag, linestatus) groups of the separate flag layout, A/O and R/O (codes
+    // 1 and 5) need a receipt date before the ship date and do not occur in TPC-H data: their rows
+    // go straight into the CTA's 128-bit shared table (red) behind one warp vote, so that only the
+    // four other groups' planes take registers (a kernel of 128 registers a thread, 12 warps).
+    static constexpr bool kCold = (G == 6) && !kWideQty;
+    static constexpr int kPlanes = kWideQty ? 1 : (kCold ? 4 : G);
     GroupRegs<kWideQty> g[kWideQty ? G : 1];      // row-wise path (uncompressed layout)
-    GroupPlanes gq[kWideQty ? 1 : G];             // quad path (compressed layouts)
-    __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
+    GroupPlanes gq[kPlanes];                      // quad path (compressed layouts)
+    unsigned long long* red;                      // the CTA's [G][6][lo, hi] table (cold groups)
+    // group of plane slot s: the codes themselves, or with cold groups AF, NF, NO, RF
+    static __device__ __forceinline__ constexpr uint32_t group_of(int s) {
+        return kCold ? (s == 0 ? 0u : (uint32_t)s + 1u) : (uint32_t)s;
+    }
+    static __device__ __forceinline__ constexpr bool cold(int grp) { return kCold && (grp == 1 || grp == 5); }
+    __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*, unsigned long long* cta_red) {
+        red = cta_red;
 #pragma unroll
         for (int i = 0; i < (kWideQty ? G : 1); ++i) g[i].zero();
 #pragma unroll
-        for (int i = 0; i < (kWideQty ? 1 : G); ++i) gq[i].zero();
+        for (int i = 0; i < kPlanes; ++i) gq[i].zero();
+    }
+    // One passing row of a cold group, exactly, into the CTA's table.
+    __device__ __forceinline__ void cold_row(uint32_t grp, uint32_t q, uint32_t d, uint32_t a, uint32_t ab,
+                                             uint32_t p) {
+        unsigned long long* v = red + 2 * (grp * kNumAggs);
+        atomic_add_u128_shared(v + 2 * kAggCount, 1, 0);
+        atomic_add_u128_shared(v + 2 * kAggQty, q, 0);
+        atomic_add_u128_shared(v + 2 * kAggBasePrice, p, 0);
+        atomic_add_u128_shared(v + 2 * kAggDisc, d, 0);
+        atomic_add_u128_shared(v + 2 * kAggDiscPrice, (uint64_t)a * p, 0);
+        atomic_add_u128_shared(v + 2 * kAggCharge, (uint64_t)ab * p, 0);
     }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
         if constexpr (kWideQty) {
 #pragma unroll
             for (int i = 0; i < G; ++i) g[i].add(c == (uint32_t)i, q, d, a, ab, p);
         } else {
+            if (kCold && (c == 1u || c == 5u)) {
+                cold_row(c, q, d, a, ab, p);
+                return;
+            }
             // one row through the quad path (tail rows)
             Quad x;
             x.OH = c < (uint32_t)G ? (1u << c) : 0u;
@@ -244,26 +272,24 @@ struct AccPerThread {
             x.ABL = ab & 0xFFu;
             x.ABH = ab >> 8;
 #pragma unroll
-            for (int i = 0; i < G; ++i) gq[i].add_quad(x.OH, (uint32_t)i, x);   // no warp vote: lanes diverge here
+            for (int i = 0; i < kPlanes; ++i) gq[i].add_quad(x.OH, group_of(i), x);   // no warp vote: lanes diverge here
         }
     }
-    // Called by all lanes of the warp. With the six (returnflag, linestatus) groups of the separate
-    // flag layout, A/O and R/O (groups 1 and 5) need a receipt date before the ship date and do
-    // not occur in TPC-H data: their planes run only when a lane of the warp has such a row.
+    // Called by all lanes of the warp.
     template <bool kTop>
     __device__ __forceinline__ void add_quad_planes(const Quad& x) {
-        if constexpr (G == 6) {
-            gq[0].template add_quad<kTop>(x.OH, 0u, x);
-            gq[2].template add_quad<kTop>(x.OH, 2u, x);
-            gq[3].template add_quad<kTop>(x.OH, 3u, x);
-            gq[4].template add_quad<kTop>(x.OH, 4u, x);
-            if (__any_sync(0xffffffffu, x.OH & 0x22222222u)) {
-                gq[1].template add_quad<kTop>(x.OH, 1u, x);
-                gq[5].template add_quad<kTop>(x.OH, 5u, x);
-            }
-        } else {
 #pragma unroll
-            for (int i = 0; i < G; ++i) gq[i].template add_quad<kTop>(x.OH, (uint32_t)i, x);
+        for (int i = 0; i < kPlanes; ++i) gq[i].template add_quad<kTop>(x.OH, group_of(i), x);
+        if constexpr (kCold) {
+            if (__any_sync(0xffffffffu, x.OH & 0x22222222u)) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const uint32_t b = (x.OH >> (8 * r)) & 0x22u;
+                    if (b)
+                        cold_row((b & 2u) ? 1u : 5u, (x.Q >> (8 * r)) & 0xFFu, (x.D >> (8 * r)) & 0xFFu, x.a[r],
+                                 x.ab[r], x.p[r]);
+                }
+            }
         }
     }
     __device__ __forceinline__ void add_quad(const Quad& x) {
@@ -279,13 +305,16 @@ struct AccPerThread {
             for (int i = 0; i < G; ++i) g[i].fold();
         }
     }
+    // plane slot of group i (not called for cold groups)
+    static __device__ __forceinline__ constexpr int slot_of(int i) { return kCold ? (i == 0 ? 0 : i - 1) : i; }
+    // The thread's partial of group i (0 for a cold group: its rows are in the CTA table already).
     __device__ __forceinline__ uint64_t value(int i, int a) const {
         if constexpr (kWideQty) return g[i].value(a);
-        else return gq[i].value(a);
+        else return cold(i) ? 0ull : gq[slot_of(i)].value(a);
     }
     __device__ __forceinline__ void zero_group(int i) {
         if constexpr (kWideQty) g[i].zero();
-        else gq[i].zero();
+        else if (!cold(i)) gq[slot_of(i)].zero();
     }
     // whether this thread sums the rows of group code c (every thread reads every row it is given)
     __device__ __forceinline__ bool owns(uint32_t) const { return true; }
@@ -297,6 +326,7 @@ struct AccPerThread {
         fold();
 #pragma unroll
         for (int i = 0; i < G; ++i) {
+            if (cold(i)) continue;
 #pragma unroll
             for (int a = 0; a < kNumAggs; ++a) {
                 uint64_t lo = value(i, a), hi = 0;
@@ -316,7 +346,7 @@ struct AccWarpLane {
     GroupRegs<kWideQty> r;
     GroupQuadRegs rq;
     uint32_t my;
-    __device__ __forceinline__ void init(uint32_t lane, uint32_t, uint8_t*) {
+    __device__ __forceinline__ void init(uint32_t lane, uint32_t, uint8_t*, unsigned long long*) {
         r.zero();
         rq.zero();
         my = lane % G;
@@ -388,7 +418,7 @@ struct AccLocal {
     static constexpr int kQtyShift = 16, kDiscShift = kWideQty ? 16 : 39;
     uint64_t t[G][kWords];   // [0] count | quantity << 16 | discount << 39 (or count | discount << 16), [1] p,
                              // [2] (100-d) p, [3] (100-d)(100+t) p, [4] quantity (reference-typed columns)
-    __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*) {
+    __device__ __forceinline__ void init(uint32_t, uint32_t, uint8_t*, unsigned long long*) {
         for (int i = 0; i < G; ++i)
             for (int j = 0; j < kWords; ++j) t[i][j] = 0;
     }
@@ -452,7 +482,7 @@ struct AccSharedPerThread {
     static constexpr int kDiscShift = kWideQty ? 16 : 39;
     uint64_t* tab;       // kWords * G * T entries: [w0, p, dp, ch, (quantity)][group][thread]
     uint32_t tid, nthreads;
-    __device__ __forceinline__ void init(uint32_t, uint32_t consumer_tid, uint8_t* scratch) {
+    __device__ __forceinline__ void init(uint32_t, uint32_t consumer_tid, uint8_t* scratch, unsigned long long*) {
         tid = consumer_tid;
         nthreads = blockDim.x - 32;
         tab = reinterpret_cast<uint64_t*>(scratch);
@@ -526,8 +556,8 @@ struct AccGlobal {
     static_assert(kGlobalFlushTiles >= 1, "flush cadence");
     AccPerThread<G, kWideQty> buf;
     uint32_t tiles;
-    __device__ __forceinline__ void init(uint32_t a, uint32_t b, uint8_t* s) {
-        buf.init(a, b, s);
+    __device__ __forceinline__ void init(uint32_t a, uint32_t b, uint8_t* s, unsigned long long* r) {
+        buf.init(a, b, s, r);
         tiles = 0;
     }
     __device__ __forceinline__ void add(uint32_t c, uint32_t q, uint32_t d, uint32_t a, uint32_t ab, uint32_t p) {
@@ -818,7 +848,7 @@ q1_scan_kernel(const __grid_constant__ ScanParams prm) {
         using Acc = typename AccSel<P, G, T::kWideQty>::T;
         const uint32_t ctid = threadIdx.x;  // 0 .. 32W-1
         Acc acc;
-        acc.init(lane, ctid, smem + S * kStage);
+        acc.init(lane, ctid, smem + S * kStage, red);
         uint32_t bad = 0;
         constexpr uint32_t kSteps = R / T::kRowsPerStep;  // steps per tile
         // Rows one consumer thread adds per tile, and how often the 16-bit packed partials
