@@ -128,9 +128,24 @@ def test_domain_edges_take_exact_paths(table, num_groups, placement):
             check(wide, keys, num_groups, cutoff, run_gpu(c, keys, num_groups, placement, cutoff))
 
 
+@pytest.mark.parametrize("rows,blocks", [(r, 1) for r in [1, 2047, 2048, 2049, 4097, 98_303, 98_304, 98_305,
+                                                           101_377, 104_449]] +
+                         [(r, 4) for r in [393_215, 393_216, 393_217]] + [(1_000_003, 0)])
+@pytest.mark.parametrize("num_groups", [4, 8])
+def test_registers_ragged_tiles(cuda, rows, blocks, num_groups):
+    """Row counts around the register planes' tiles: four groups' planes take 12 consumer warps
+    over 3072-row tiles on a table of at least 32 tiles per CTA (98,304 rows for one CTA, 393,216
+    for four), 8 warps over 2048-row tiles below that; eight groups' planes always the latter."""
+    part = gen_np.compress(gen_np.generate(SEED + 6, 0, rows))
+    c, keep = device_cols(part)
+    keys = gen_np.group_keys_uniform(SEED + 5, 0, rows, num_groups)
+    check(part, keys, num_groups, 729999,
+          run_gpu(c, keys, num_groups, "in_registers_per_thread", 729999, blocks=blocks))
+
+
 @pytest.fixture(scope="module")
 def long_table(cuda):
-    rows = 9_000_011
+    rows = 13_000_011
     comp = widen(gen_np.compress(gen_np.generate(SEED + 1, 0, rows)), 99, frac=0.001)
     c, keep = device_cols(comp)
     return comp, c, keep, rows
@@ -140,8 +155,8 @@ def long_table(cuda):
     (4, "in_registers_per_thread"), (8, "in_registers_per_thread"), (64, "shared_mem_per_thread"),
     (200, "shared_mem_per_thread"), (1024, "shared_mem_per_thread"), (5000, "shared_mem_per_thread")])
 def test_one_cta_flushes_mid_launch(long_table, num_groups, placement):
-    """One CTA over 9M rows: the per-thread planes (every 4032 tiles) and the shared tables
-    (every 2^23 rows) are flushed inside the launch."""
+    """One CTA over 13M rows: the per-thread planes (every 4032 tiles of 3072 or 2048 rows) and the
+    shared tables (every 2^23 rows) are flushed inside the launch."""
     comp, c, _, rows = long_table
     keys = gen_np.group_keys_uniform(SEED + 2, 0, rows, num_groups)
     check(comp, keys, num_groups, 729999, run_gpu(c, keys, num_groups, placement, 729999, blocks=1))

@@ -43,19 +43,24 @@ using namespace ptx;
 
 namespace gk {
 
-constexpr uint32_t R = ka::R;         // rows per tile
 constexpr uint32_t kMaxStages = 4;    // ring stages (3 when the table needs the room)
 constexpr uint32_t kWideSlots = 4096; // slot-table keys of the single-pass kernel
 constexpr uint32_t kChooseAbove = 256; // the shared placement's path is chosen on the device above
 constexpr uint32_t kMaxDynSmem = 227 * 1024;
-// consumer warps: 8 for the register planes (128 registers a thread), 16 for the shared-table and
-// global placements, whose atomics need more warps in flight to hide their latency
-template <int P>
-__host__ __device__ constexpr uint32_t consumer_warps() { return P == kPlaceInRegistersPerThread ? 8u : 16u; }
-constexpr uint32_t kStage = ka::kStageBytes;
-constexpr uint32_t kSteps = R / 4;    // 4 rows per consumer step
-static_assert(kSteps % (16 * 32) == 0, "steps must divide evenly");
-static_assert(kStage % 16 == 0, "stage alignment");
+// Consumer warps: 16 for the shared-table and global placements, whose atomics need many warps in
+// flight to hide their latency; 8 for the register planes, or 12 for four groups' planes on a large
+// table (kWide: their 127 registers a thread fit the 128 that 13 warps leave, and a third warp per
+// scheduler hides more of the planes' issue latency: 600 M rows 1.49 -> 1.24 ms, 80% -> 96% of HBM).
+template <int P, int NG, bool kWide>
+__host__ __device__ constexpr uint32_t consumer_warps() {
+    return P == kPlaceInRegistersPerThread ? ((NG <= 4 && kWide) ? 12u : 8u) : 16u;
+}
+// Rows per tile: 2048, or 3072 with 12 warps, so that every consumer thread takes two quads of a
+// tile (at most 8 rows, which the planes' flush cadence assumes).
+template <int P, int NG, bool kWide>
+__host__ __device__ constexpr uint32_t tile_rows() { return consumer_warps<P, NG, kWide>() == 12u ? 3072u : ka::R; }
+template <int P, int NG, bool kWide>
+__host__ __device__ constexpr uint32_t stage_bytes() { return ka::TileLayout<tile_rows<P, NG, kWide>()>::kStageBytes; }
 
 // Table engine of the shared_mem_per_thread placement.
 enum TableKind : uint32_t { kTableNone = 0, kTableCube = 1, kTableSlots = 2, kTableCube3 = 3 };
@@ -74,9 +79,11 @@ __host__ __device__ constexpr uint32_t table_bytes(uint32_t kind, uint32_t num_g
                                                                                                  : kWideSlots)
                                                                             : 0u));
 }
+// (tables live only beside 2048-row stages; the register planes' 3072-row stages take 4 x 39 KB)
 __host__ __device__ constexpr uint32_t ring_stages(uint32_t kind, uint32_t num_groups) {
     return kMaxStages * ka::kStageBytes + table_bytes(kind, num_groups) <= kMaxDynSmem ? kMaxStages : kMaxStages - 1;
 }
+static_assert(kMaxStages * ka::TileLayout<3072>::kStageBytes + 512 <= kMaxDynSmem, "register-plane ring");
 // the largest tables fit beside a 3-stage ring, with room left for the static shared memory
 static_assert((kMaxStages - 1) * ka::kStageBytes + ka::cube_bytes(ka::kCubeMaxGroups) + 512 <= kMaxDynSmem,
               "1024-group cells");
@@ -97,12 +104,18 @@ struct GroupKeyParams {
     uint32_t mode_want;
 };
 
-// P: placement; NG: plane groups of in_registers_per_thread (4 or 8).
-template <int P, int NG>
-__global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
+// P: placement; NG: plane groups of in_registers_per_thread (4 or 8); kWide: 12 consumer warps
+// over 3072-row tiles for four groups' planes.
+template <int P, int NG, bool kWide = false>
+__global__ void __launch_bounds__((gk::consumer_warps<P, NG, kWide>() + 1) * 32, 1)
     q1_groupkey_kernel(const __grid_constant__ GroupKeyParams prm) {
     using namespace gk;
-    constexpr uint32_t W = consumer_warps<P>();
+    constexpr uint32_t W = consumer_warps<P, NG, kWide>();
+    constexpr uint32_t R = tile_rows<P, NG, kWide>();
+    constexpr uint32_t kStage = stage_bytes<P, NG, kWide>();
+    constexpr uint32_t kSteps = R / 4;   // 4 rows per consumer step
+    static_assert(kSteps % (W * 32) == 0 && kSteps / (W * 32) * 4 <= 8, "two quads per consumer thread at most");
+    static_assert(P == kPlaceInRegistersPerThread || R == ka::R, "tables beside 2048-row stages only");
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t full_bar[kMaxStages];
     __shared__ __align__(8) uint64_t empty_bar[kMaxStages];
@@ -150,8 +163,9 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
                 mbar_arrive_expect_tx(fb, kStage);
 #pragma unroll
                 for (int c = 0; c < 6; ++c)
-                    bulk_g2s(ring + s * kStage + ka::col_off(c), prm.col[c] + t * (uint64_t)ka::col_bytes(c),
-                             ka::col_bytes(c), fb, pol);
+                    bulk_g2s(ring + s * kStage + ka::TileLayout<R>::col_off(c),
+                             prm.col[c] + t * (uint64_t)ka::TileLayout<R>::col_bytes(c),
+                             ka::TileLayout<R>::col_bytes(c), fb, pol);
                 if (++s == S) {
                     s = 0;
                     ph ^= 1u;
@@ -219,7 +233,7 @@ __global__ void __launch_bounds__((gk::consumer_warps<P>() + 1) * 32, 1)
             const uint32_t base = ring + s * kStage;
 #pragma unroll
             for (uint32_t it = 0; it < kSteps / (W * 32); ++it)
-                add_quad(ka::load_quad(base, ctid + it * (W * 32), prm.cutoff, bad));
+                add_quad(ka::load_quad<R>(base, ctid + it * (W * 32), prm.cutoff, bad));
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&empty_bar[s]));
             if (++s == S) {
@@ -266,19 +280,20 @@ __global__ void __launch_bounds__(256) q1_groupkey_finalize(const unsigned long 
     atomic_add_u128(o + 2 * kAggCharge, (uint64_t)ch, (uint64_t)(ch >> 64));
 }
 
-template <int P, int NG>
+template <int P, int NG, bool kWide = false>
 static cudaError_t launch_gk(const GroupKeyParams& prm, int sm_count, int max_blocks, cudaStream_t st) {
     using namespace gk;
-    const uint32_t dyn = prm.stages * kStage + table_bytes(prm.table, prm.num_groups);
-    cudaError_t e =
-        cudaFuncSetAttribute(q1_groupkey_kernel<P, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    constexpr uint32_t R = tile_rows<P, NG, kWide>();
+    const uint32_t dyn = prm.stages * stage_bytes<P, NG, kWide>() + table_bytes(prm.table, prm.num_groups);
+    cudaError_t e = cudaFuncSetAttribute(q1_groupkey_kernel<P, NG, kWide>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     const uint64_t tiles = prm.rows / R;
     uint64_t blocks = tiles ? tiles : 1;
     uint64_t cap = (uint64_t)sm_count;
     if (max_blocks > 0 && (uint64_t)max_blocks < cap) cap = (uint64_t)max_blocks;
     if (blocks > cap) blocks = cap;
-    q1_groupkey_kernel<P, NG><<<(unsigned)blocks, (consumer_warps<P>() + 1) * 32, dyn, st>>>(prm);
+    q1_groupkey_kernel<P, NG, kWide><<<(unsigned)blocks, (consumer_warps<P, NG, kWide>() + 1) * 32, dyn, st>>>(prm);
     return cudaGetLastError();
 }
 
@@ -396,10 +411,19 @@ cudaError_t launch_groupkey(int placement, const uint8_t* const cols[6], uint64_
             if ((e = launch_gk<kPlaceGlobal, 4>(g, sm_count, max_blocks, stream)) != cudaSuccess) return e;
         }
         switch (placement) {
-            case kPlaceInRegistersPerThread:
-                e = num_groups <= 4 ? launch_gk<kPlaceInRegistersPerThread, 4>(prm, sm_count, max_blocks, stream)
-                                    : launch_gk<kPlaceInRegistersPerThread, 8>(prm, sm_count, max_blocks, stream);
+            case kPlaceInRegistersPerThread: {
+                // The wide tiles on a table of at least 32 tiles per CTA of the grid (14.5 M rows on
+                // 148 SMs): one such scan is up to 20% faster (50 M rows 136 -> 115 us), but a queue
+                // of launches on tables of a few million rows ran slower with them (256 launches on
+                // 10^4..5*10^7 rows: 10.72 ms with 2048-row tiles throughout, 11.56 ms with the wide
+                // ones from 2 tiles per CTA, 10.78 ms from 32).
+                const uint64_t grid = (max_blocks > 0 && max_blocks < sm_count) ? (uint64_t)max_blocks : (uint64_t)sm_count;
+                const bool wide = n >= 32 * grid * gk::tile_rows<kPlaceInRegistersPerThread, 4, true>();
+                e = num_groups > 4 ? launch_gk<kPlaceInRegistersPerThread, 8>(prm, sm_count, max_blocks, stream)
+                    : wide         ? launch_gk<kPlaceInRegistersPerThread, 4, true>(prm, sm_count, max_blocks, stream)
+                                   : launch_gk<kPlaceInRegistersPerThread, 4>(prm, sm_count, max_blocks, stream);
                 break;
+            }
             case kPlaceSharedMemPerThread: e = launch_gk<kPlaceSharedMemPerThread, 4>(prm, sm_count, max_blocks, stream); break;
             case kPlaceGlobal: e = launch_gk<kPlaceGlobal, 4>(prm, sm_count, max_blocks, stream); break;
             default: return cudaErrorInvalidValue;

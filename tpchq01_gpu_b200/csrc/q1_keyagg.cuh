@@ -50,19 +50,34 @@ namespace ka {
 using namespace ptx;
 
 // ---------------------------------------------------------------------------------------------
-// Tile layout (R rows per tile, every column offset a multiple of 16 bytes)
+// Tile layout (TR rows per tile, TR a multiple of 16, so every column offset is a multiple of 16
+// bytes): ship u16 | qty u8 | disc u8 | tax u8 | price u32 | key u32
 // ---------------------------------------------------------------------------------------------
+template <uint32_t TR>
+struct TileLayout {
+    static_assert(TR % 16 == 0, "column offsets must stay 16-byte aligned");
+    static constexpr uint32_t kOffShip = 0, kOffQty = 2 * TR, kOffDisc = 3 * TR, kOffTax = 4 * TR,
+                              kOffPrice = 5 * TR, kOffKey = 9 * TR;
+    static constexpr uint32_t kStageBytes = 13 * TR;
+    static __host__ __device__ constexpr uint32_t col_bytes(int c) { return c == 0 ? 2 * TR : (c < 4 ? TR : 4 * TR); }
+    static __host__ __device__ constexpr uint32_t col_off(int c) {
+        return c == 0 ? kOffShip
+                      : (c == 1 ? kOffQty : (c == 2 ? kOffDisc : (c == 3 ? kOffTax : (c == 4 ? kOffPrice : kOffKey))));
+    }
+};
+// The 2048-row tile of the batch kernels, the partitioned path and the group-key kernel's table
+// and global placements.
 constexpr uint32_t R = 2048;
-constexpr uint32_t kOffShip = 0, kOffQty = 2 * R, kOffDisc = 3 * R, kOffTax = 4 * R, kOffPrice = 5 * R,
-                   kOffKey = 9 * R;
-constexpr uint32_t kStageBytes = 13 * R;
-__host__ __device__ constexpr uint32_t col_bytes(int c) { return c == 0 ? 2 * R : (c < 4 ? R : 4 * R); }
-__host__ __device__ constexpr uint32_t col_off(int c) {
-    return c == 0 ? kOffShip : (c == 1 ? kOffQty : (c == 2 ? kOffDisc : (c == 3 ? kOffTax : (c == 4 ? kOffPrice : kOffKey))));
-}
+constexpr uint32_t kOffShip = TileLayout<R>::kOffShip, kOffQty = TileLayout<R>::kOffQty,
+                   kOffDisc = TileLayout<R>::kOffDisc, kOffTax = TileLayout<R>::kOffTax,
+                   kOffPrice = TileLayout<R>::kOffPrice, kOffKey = TileLayout<R>::kOffKey;
+constexpr uint32_t kStageBytes = TileLayout<R>::kStageBytes;
+__host__ __device__ constexpr uint32_t col_bytes(int c) { return TileLayout<R>::col_bytes(c); }
+__host__ __device__ constexpr uint32_t col_off(int c) { return TileLayout<R>::col_off(c); }
 
 // Flush cadences. Plane partials: at most 2^15 rows per thread; every consumer thread handles at
-// most R / 256 = 8 rows of a tile, so 4032 tiles leave room for one more partial tile.
+// most 8 rows of a tile (the kernels assert it), so 4032 tiles leave room for one more partial
+// tile.
 // Shared tables: at most 2^23 rows per CTA between flushes keeps every packed field and carry
 // word below its limit (count < 2^24 per cell; carry words < 2^32).
 constexpr uint32_t kPlaneFlushTiles = 4032;
@@ -149,16 +164,18 @@ struct KeyQuad {
     uint32_t k[4];
 };
 
-// Rows 4j..4j+3 of the tile at shared address `base`. `bad` becomes nonzero for a value outside
-// the compressed domain (ship offset > 32767, discount > 100).
+// Rows 4j..4j+3 of the TR-row tile at shared address `base`. `bad` becomes nonzero for a value
+// outside the compressed domain (ship offset > 32767, discount > 100).
+template <uint32_t TR = R>
 __device__ __forceinline__ KeyQuad load_quad(uint32_t base, uint32_t j, int32_t cut, uint32_t& bad) {
+    using TL = TileLayout<TR>;
     KeyQuad x;
-    x.PM = quad_pass_mask(lds_v2(base + kOffShip + 8 * j), cut, bad);
-    x.Q = lds_u32(base + kOffQty + 4 * j);
-    x.D = lds_u32(base + kOffDisc + 4 * j);
-    x.X = lds_u32(base + kOffTax + 4 * j);
-    const uint4 P = lds_v4(base + kOffPrice + 16 * j);
-    const uint4 K = lds_v4(base + kOffKey + 16 * j);
+    x.PM = quad_pass_mask(lds_v2(base + TL::kOffShip + 8 * j), cut, bad);
+    x.Q = lds_u32(base + TL::kOffQty + 4 * j);
+    x.D = lds_u32(base + TL::kOffDisc + 4 * j);
+    x.X = lds_u32(base + TL::kOffTax + 4 * j);
+    const uint4 P = lds_v4(base + TL::kOffPrice + 16 * j);
+    const uint4 K = lds_v4(base + TL::kOffKey + 16 * j);
     bad |= disc_out_of_domain4(x.D);
     x.p[0] = P.x, x.p[1] = P.y, x.p[2] = P.z, x.p[3] = P.w;
     x.k[0] = K.x, x.k[1] = K.y, x.k[2] = K.z, x.k[3] = K.w;
