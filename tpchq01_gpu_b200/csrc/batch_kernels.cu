@@ -114,7 +114,7 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
     };
     auto add = [&](const ka::KeyQuad& x) {
         if constexpr (E == kEngRegisters) {
-            regs.add(x, c.num_groups, bad);
+            regs.add(x, c.num_groups, c.acc, bad);
         } else if constexpr (E == kEngCube3) {
             ka::table_quad(cube3, x, c.num_groups, c.hot, c.acc, bad);
         } else if constexpr (E == kEngCube) {

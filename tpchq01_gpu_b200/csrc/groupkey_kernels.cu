@@ -185,7 +185,7 @@ __global__ void __launch_bounds__((gk::consumer_warps<P, NG, kWide>() + 1) * 32,
         // one decoded quad into the placement's engine
         auto add_quad = [&](const ka::KeyQuad& x) {
             if constexpr (P == kPlaceInRegistersPerThread) {
-                regs.add(x, G, bad);
+                regs.add(x, G, prm.acc, bad);
             } else if constexpr (P == kPlaceSharedMemPerThread) {
                 if (prm.table == kTableCube3) ka::table_quad(cube3, x, G, G, prm.acc, bad);
                 else if (prm.table == kTableCube) ka::table_quad(cube, x, G, G, prm.acc, bad);

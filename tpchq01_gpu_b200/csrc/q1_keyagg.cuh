@@ -214,12 +214,17 @@ __device__ __forceinline__ KeyQuad load_row(const uint8_t* const col[6], uint64_
 // ---------------------------------------------------------------------------------------------
 template <int NG>
 struct PlaneRegs {
-    GroupPlanes g[NG];
+    // Three price byte planes a group: a passing row with a price >= 2^24 (none in TPC-H data) is
+    // added, exactly, straight into the scratch behind one warp vote, so that eight groups' planes
+    // fit in registers (the fourth plane took 32 more a thread and made the 8-group kernel spill).
+    GroupPlanesT<3> g[NG];
     __device__ __forceinline__ void zero() {
 #pragma unroll
         for (int i = 0; i < NG; ++i) g[i].zero();
     }
-    __device__ __forceinline__ void add(const KeyQuad& kq, uint32_t num_groups, uint32_t& bad) {
+    // Every lane of the warp calls it (warp vote).
+    __device__ __forceinline__ void add(const KeyQuad& kq, uint32_t num_groups, unsigned long long* acc,
+                                        uint32_t& bad) {
         uint32_t OH = 0;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
@@ -235,8 +240,18 @@ struct PlaneRegs {
 #pragma unroll
         for (int r = 0; r < 4; ++r) x.p[r] = kq.p[r];
         quad_derive(x, kq.X);
+        if (__any_sync(0xffffffffu, x.P[3])) {
 #pragma unroll
-        for (int i = 0; i < NG; ++i) g[i].add_quad(x.OH, (uint32_t)i, x);
+            for (int r = 0; r < 4; ++r) {
+                if (((x.P[3] >> (8 * r)) & 0xFFu) && ((x.OH >> (8 * r)) & 0xFFu)) {
+                    scratch_row(acc, kq.k[r], (kq.Q >> (8 * r)) & 0xFFu, (kq.D >> (8 * r)) & 0xFFu,
+                                (kq.X >> (8 * r)) & 0xFFu, kq.p[r]);
+                    x.OH &= ~(0xFFu << (8 * r));
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NG; ++i) g[i].template add_quad<false>(x.OH, (uint32_t)i, x);
     }
     // Warp sums of the per-thread partials into the scratch; every lane of the warp calls it.
     __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t lane) {

@@ -39,14 +39,16 @@ __device__ __forceinline__ void byte_planes(const uint32_t w[4], uint32_t out[4]
 //   sum (100-d)(100+t) p  sum_k 2^8k (dp4a(ABL & M, P_k) + 2^8 dp4a(ABH & M, P_k))
 // Every 32-bit partial stays exact while a thread adds at most 2^15 rows per launch (the host
 // caps launches accordingly): the largest, an ab-low plane, grows by <= 4*255*255 per quad.
-// A quad whose four prices are below 2^24 has a zero top plane and may skip its 4 dp4a.
-struct GroupPlanes {
+// kPlanes = 4 covers every 32-bit price; with kPlanes = 3 the caller keeps rows with a price
+// >= 2^24 out of the planes (they need the top byte plane).
+template <int kPlanes>
+struct GroupPlanesT {
     uint32_t cnt, q, d;
-    uint32_t p[4], dp[4], chl[4], chh[4];
+    uint32_t p[kPlanes], dp[kPlanes], chl[kPlanes], chh[kPlanes];
     __device__ __forceinline__ void zero() {
         cnt = q = d = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) p[k] = dp[k] = chl[k] = chh[k] = 0;
+        for (int k = 0; k < kPlanes; ++k) p[k] = dp[k] = chl[k] = chh[k] = 0;
     }
     // kTop: the prices' top byte plane may be nonzero. Callers pass false when no lane of the
     // warp has a price >= 2^24 in the quad (TPC-H prices stay below 2^24): 15 dp4a instead of 19.
@@ -59,7 +61,7 @@ struct GroupPlanes {
         q = __dp4a(W1, x.Q, q);
         d = __dp4a(W1, x.D, d);
 #pragma unroll
-        for (int k = 0; k < (kTop ? 4 : 3); ++k) {
+        for (int k = 0; k < ((kTop && kPlanes == 4) ? 4 : 3); ++k) {
             p[k] = __dp4a(W1, x.P[k], p[k]);
             dp[k] = __dp4a(MA, x.P[k], dp[k]);
             chl[k] = __dp4a(ML, x.P[k], chl[k]);
@@ -74,19 +76,20 @@ struct GroupPlanes {
             case kAggDisc: return d;
             case kAggBasePrice:
 #pragma unroll
-                for (int k = 0; k < 4; ++k) v += (uint64_t)p[k] << (8 * k);
+                for (int k = 0; k < kPlanes; ++k) v += (uint64_t)p[k] << (8 * k);
                 return v;
             case kAggDiscPrice:
 #pragma unroll
-                for (int k = 0; k < 4; ++k) v += (uint64_t)dp[k] << (8 * k);
+                for (int k = 0; k < kPlanes; ++k) v += (uint64_t)dp[k] << (8 * k);
                 return v;
             default:
 #pragma unroll
-                for (int k = 0; k < 4; ++k) v += ((uint64_t)chl[k] << (8 * k)) + ((uint64_t)chh[k] << (8 * k + 8));
+                for (int k = 0; k < kPlanes; ++k) v += ((uint64_t)chl[k] << (8 * k)) + ((uint64_t)chh[k] << (8 * k + 8));
                 return v;
         }
     }
 };
+using GroupPlanes = GroupPlanesT<4>;
 
 
 // Any byte of a discount word above 100 (top bit of (b & 0x7F) + 27, or b >= 128).
