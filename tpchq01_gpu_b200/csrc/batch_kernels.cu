@@ -90,7 +90,7 @@ __device__ __forceinline__ bool consume_engine(const BatchParams& prm, uint32_t 
     const uint32_t lane = threadIdx.x & 31u, ctid = threadIdx.x;
     ka::PlaneRegs<4> regs;
     ka::Cube3Table cube3;
-    ka::CubeTable cube;
+    ka::CubeTableT<false> cube;
     ka::SlotTable slots;
     if constexpr (E == kEngRegisters) regs.zero();
     Current c{nullptr, nullptr, 0xFFFFFFFFu, 0, 0, 0};

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__((gk::consumer_warps<P, NG, kWide>() + 1) * 32,
     const uint32_t ring = smem_addr(smem);
     const uint32_t G = prm.num_groups;
     ka::Cube3Table cube3;
-    ka::CubeTable cube;
+    ka::CubeTableT<true> cube;
     ka::SlotTable slots;
     const uint32_t hot = G < kWideSlots ? G : kWideSlots;
     if (P == kPlaceSharedMemPerThread) {

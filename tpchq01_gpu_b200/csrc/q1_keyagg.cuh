@@ -10,8 +10,8 @@
 //   Cube3Table     num_groups <= 64: a shared-memory table per (group, discount, tax) cell; a
 //                  row adds its count, its quantity and its price: three atomics.
 //   CubeTable      num_groups <= 1024: a shared-memory table per (group, discount) cell. A row
-//                  adds its count, price and tax * price to its cell and its quantity to one of
-//                  its group's four words; the discounted sums follow exactly at the flush, because the
+//                  adds its count, price and tax * price to its cell and its quantity to its
+//                  group's word; the discounted sums follow exactly at the flush, because the
 //                  discount of a cell is known there: sum (100-d) p = sum_d (100-d) P_d and
 //                  sum (100-d)(100+t) p = sum_d (100-d) (100 P_d + TP_d).
 //   SlotTable      one shared-memory slot per key below the table's size (2048 in the batch
@@ -28,8 +28,11 @@
 // and the (group, discount, tax) cube keep them as (low word, carry word) pairs: the low word's
 // atomic returns the old value, and a wrap adds the carry to the high word. The
 // (group, discount) cube keeps only the low words of its cells, so that 1024 groups fit: a wrap of
-// a price or tax-price word (a few rows in a thousand) adds its 2^32 straight to the group's
-// scratch sums, where the cell's discount fixes what it is worth in each. Rows
+// a price or tax-price word (a few rows in a thousand) is counted in three words of its group
+// (wraps, and the cells' 100 - d summed over price and over tax-price wraps), from which the
+// flush adds what the wraps are worth. (Sending each wrap's 2^32 straight to the group's scratch
+// sums in global memory serialised on the L2 when one key holds many rows: Zipf keys over 1024
+// groups at full pass 2.98 ms per 600 M rows, 1.57 ms without those global atomics.) Rows
 // outside the tables' fast domain
 // (discount > 10, tax > 8 or price >= 2^24; TPC-H data has none) take the global path, so every
 // result is exact over the whole compressed domain.
@@ -92,10 +95,10 @@ constexpr uint32_t kCube3Words = 4;         // count, quantity, price low, price
 constexpr uint32_t kSlots = 2048;
 constexpr uint32_t kSlotWords = 9;          // count, discount, quantity, price lo/hi, discount x price lo/hi, charge lo/hi
 
-// cells, then (CubeTable) kCubeQtyWays quantity words per group
-constexpr uint32_t kCubeQtyWays = 4;
+// cells, then (CubeTable) kCubeGroupWords words per group: quantity and three wrap counters
+constexpr uint32_t kCubeGroupWords = 4;
 __host__ __device__ constexpr uint32_t cube_bytes(uint32_t num_groups) {
-    return num_groups * (kCubeDisc * kCubeWords + kCubeQtyWays) * 4;
+    return num_groups * (kCubeDisc * kCubeWords + kCubeGroupWords) * 4;
 }
 __host__ __device__ constexpr uint32_t cube3_bytes(uint32_t num_groups) {
     return num_groups * kCubeDisc * kCubeTax * kCube3Words * 4;
@@ -132,15 +135,6 @@ __device__ __forceinline__ void scratch_row(unsigned long long* acc, uint32_t ke
 
 __device__ __forceinline__ bool fast_domain(uint32_t d, uint32_t t, uint32_t p) {
     return d < kCubeDisc && t <= 8u && p < (1u << 24);
-}
-
-// A wrap of a (group, discount) cell's 32-bit price word: 2^32 of price, a 2^32 of disc_price and
-// ab = 100 a 2^32 of charge (a = 100 - d).
-__device__ __forceinline__ void carry_price(unsigned long long* acc, uint32_t g, uint32_t a, uint32_t ab) {
-    unsigned long long* s = acc + 8ull * g;
-    red_add(s + 3, 1ull << 32);
-    red_add(s + 5, a);
-    red_add(s + 7, ab);
 }
 
 // 64-bit sum as (lo, hi) 32-bit shared words: lo += v, carry into hi.
@@ -274,26 +268,37 @@ struct PlaneRegs {
 // ---------------------------------------------------------------------------------------------
 // CubeTable: shared (group, discount) cells
 // ---------------------------------------------------------------------------------------------
-struct CubeTable {
-    uint32_t* w;       // [kCubeWords][cells]: count, price, tax * price
-    uint32_t* qg;      // [groups][kCubeQtyWays]: quantity, a row's in word (discount & 3), so that the
-                       // rows of a frequent key spread their atomics over four words
-    uint32_t cells;
+// kSharedCarries: wraps counted in the group's shared words (the group-key kernel); otherwise
+// each wrap's worth goes straight to the group's scratch sums and the group's four words hold its
+// quantity four ways, by discount & 3 (the batch kernel, whose combined engines measured 4-5% slower
+// with the shared counters although its 1024-group instances do not contend: 256 instances 4.02
+// -> 4.20 ms).
+template <bool kSharedCarries>
+struct CubeTableT {
+    uint32_t* w;       // [kCubeWords][cells]: count, price, tax * price (low words)
+    uint32_t* gw;      // kSharedCarries: [kCubeGroupWords][groups], word-major (consecutive groups'
+                       // words in consecutive banks): quantity; wraps of the group's cells' price
+                       // words; sum (100 - d) over those wraps; sum (100 - d) over wraps of tax *
+                       // price words. Otherwise [groups][kCubeGroupWords]: quantity by discount & 3.
+    uint32_t cells, groups;
     __device__ __forceinline__ void bind(uint8_t* base, uint32_t num_groups) {
         w = reinterpret_cast<uint32_t*>(base);
         cells = num_groups * kCubeDisc;
-        qg = w + kCubeWords * cells;
+        groups = num_groups;
+        gw = w + kCubeWords * cells;
     }
     __device__ __forceinline__ void zero(uint32_t tid, uint32_t nthreads) {
-        for (uint32_t i = tid; i < kCubeWords * cells + kCubeQtyWays * (cells / kCubeDisc); i += nthreads) w[i] = 0;
+        for (uint32_t i = tid; i < kCubeWords * cells + kCubeGroupWords * groups; i += nthreads) w[i] = 0;
     }
     // Rows r of a quad with bit r of `m` set (passing, key < num_groups, fast domain). All
     // atomics of the quad are issued before any carry is checked, so their latencies overlap.
     static constexpr bool kPacked = true;
-    // The quantity, discount and tax bytes of the four rows packed in Q, D, X; acc: the scratch
-    // that takes the price words' wraps. A cell's count and a group's quantity cannot wrap
-    // between flushes (at most 2^23 rows per CTA: count < 2^24, quantity <= 255 * 2^23 < 2^32),
-    // so their atomics need no result.
+    // The quantity, discount and tax bytes of the four rows packed in Q, D, X; acc: the scratch. A
+    // cell's count and a group's quantity cannot wrap between flushes (at most 2^23 rows per CTA:
+    // count < 2^24, quantity <= 255 * 2^23 < 2^32), so their atomics need no result. A wrap of a
+    // cell's price or tax * price word (a few rows in a thousand) is worth, with the cell's
+    // discount d and a = 100 - d, 2^32 of price, 2^32 a of disc_price and 2^32 100 a of charge,
+    // or 2^32 a of charge.
     __device__ __forceinline__ void add_quad_packed(uint32_t m, const uint32_t key[4], uint32_t Q, uint32_t D,
                                                     uint32_t X, const uint32_t p[4], unsigned long long* acc) {
         uint32_t c[4], vt[4], op[4], ot[4];
@@ -305,7 +310,10 @@ struct CubeTable {
             op[r] = ot[r] = 0;
             if ((m >> r) & 1u) {
                 atomicAdd(w + c[r], 1u);
-                atomicAdd(qg + key[r] * kCubeQtyWays + ((D >> (8 * r)) & 3u), (Q >> (8 * r)) & 0xFFu);
+                if constexpr (kSharedCarries)
+                    atomicAdd(gw + key[r], (Q >> (8 * r)) & 0xFFu);
+                else
+                    atomicAdd(gw + key[r] * kCubeGroupWords + ((D >> (8 * r)) & 3u), (Q >> (8 * r)) & 0xFFu);
                 op[r] = atomicAdd(w + cells + c[r], p[r]);
                 ot[r] = atomicAdd(w + 2 * cells + c[r], vt[r]);
             }
@@ -319,21 +327,42 @@ struct CubeTable {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const uint32_t a = 100u - ((D >> (8 * r)) & 0xFFu);
-                if (op[r] > ~p[r]) carry_price(acc, key[r], a, 100u * a);
-                if (ot[r] > ~vt[r]) red_add(acc + 8ull * key[r] + 7, a);
+                if constexpr (kSharedCarries) {
+                    uint32_t* g = gw + key[r];
+                    if (op[r] > ~p[r]) {
+                        atomicAdd(g + groups, 1u);
+                        atomicAdd(g + 2 * groups, a);
+                    }
+                    if (ot[r] > ~vt[r]) atomicAdd(g + 3 * groups, a);
+                } else {
+                    unsigned long long* sg = acc + 8ull * key[r];
+                    if (op[r] > ~p[r]) {
+                        red_add(sg + 3, 1ull << 32);
+                        red_add(sg + 5, a);
+                        red_add(sg + 7, 100u * a);
+                    }
+                    if (ot[r] > ~vt[r]) red_add(sg + 7, a);
+                }
             }
         }
     }
     // Cells -> per-group sums -> scratch; the caller synchronises the consumers around it.
     __device__ __forceinline__ void flush(unsigned long long* acc, uint32_t num_groups, uint32_t tid, uint32_t nthreads) {
         for (uint32_t g = tid; g < num_groups; g += nthreads) {
-            uint64_t cnt = 0, q = 0, dsum = 0, P = 0;
-            unsigned __int128 DP = 0, CH = 0;
+            uint64_t q = 0, pw = 0, aw = 0, tw = 0;
+            if constexpr (kSharedCarries) {
+                q = gw[g], pw = gw[groups + g], aw = gw[2 * groups + g], tw = gw[3 * groups + g];
 #pragma unroll
-            for (uint32_t j = 0; j < kCubeQtyWays; ++j) {
-                q += qg[g * kCubeQtyWays + j];
-                qg[g * kCubeQtyWays + j] = 0;
+                for (uint32_t j = 0; j < kCubeGroupWords; ++j) gw[j * groups + g] = 0;
+            } else {
+#pragma unroll
+                for (uint32_t j = 0; j < kCubeGroupWords; ++j) {
+                    q += gw[g * kCubeGroupWords + j];
+                    gw[g * kCubeGroupWords + j] = 0;
+                }
             }
+            uint64_t cnt = 0, dsum = 0, P = pw << 32;
+            unsigned __int128 DP = (unsigned __int128)aw << 32, CH = (unsigned __int128)(100u * aw + tw) << 32;
 #pragma unroll
             for (uint32_t d = 0; d < kCubeDisc; ++d) {
                 const uint32_t c = g * kCubeDisc + d;
