@@ -162,6 +162,16 @@ def test_one_cta_flushes_mid_launch(long_table, num_groups, placement):
     check(comp, keys, num_groups, 729999, run_gpu(c, keys, num_groups, placement, 729999, blocks=1))
 
 
+@pytest.mark.parametrize("num_groups", [64, 1024])
+def test_one_cta_zipf_keys_wrap_cells_often(long_table, num_groups):
+    """One CTA over 13M rows of Zipf keys: the most frequent key's cells collect a fifth of the rows,
+    so their 32-bit price and tax-price words wrap thousands of times between flushes; the wraps are
+    counted in the group's shared words (1024 groups) or the cell's carry word (64 groups)."""
+    comp, c, _, rows = long_table
+    keys = gen_np.group_keys_cdf(SEED + 3, 0, rows, zipf_cdf(num_groups))
+    check(comp, keys, num_groups, 740000, run_gpu(c, keys, num_groups, "shared_mem_per_thread", 740000, blocks=1))
+
+
 def test_registers_refuse_many_groups(table):
     comp, c, _ = table
     keys, _ = keys_for(64, "uniform")
