@@ -6,12 +6,14 @@
 //
 // Engines (one per placement):
 //   PlaneRegs<NG>  num_groups <= NG (4 or 8): per-thread byte-plane dot products (dp4a), four
-//                  rows per instruction, as in the scan kernel; no atomics until a flush.
+//                  rows per instruction, as in the scan kernel, over three price byte planes (a
+//                  row with a price >= 2^24 goes to the global path); no atomics until a flush.
 //   Cube3Table     num_groups <= 64: a shared-memory table per (group, discount, tax) cell; a
 //                  row adds its count, its quantity and its price: three atomics.
-//   CubeTable      num_groups <= 1024: a shared-memory table per (group, discount) cell. A row
+//   CubeTableT     num_groups <= 1024: a shared-memory table per (group, discount) cell. A row
 //                  adds its count, price and tax * price to its cell and its quantity to its
-//                  group's word; the discounted sums follow exactly at the flush, because the
+//                  group's word (the batch kernel's form: to one of four by discount & 3); the
+//                  discounted sums follow exactly at the flush, because the
 //                  discount of a cell is known there: sum (100-d) p = sum_d (100-d) P_d and
 //                  sum (100-d)(100+t) p = sum_d (100-d) (100 P_d + TP_d).
 //   SlotTable      one shared-memory slot per key below the table's size (2048 in the batch
@@ -32,7 +34,8 @@
 // (wraps, and the cells' 100 - d summed over price and over tax-price wraps), from which the
 // flush adds what the wraps are worth. (Sending each wrap's 2^32 straight to the group's scratch
 // sums in global memory serialised on the L2 when one key holds many rows: Zipf keys over 1024
-// groups at full pass 2.98 ms per 600 M rows, 1.57 ms without those global atomics.) Rows
+// groups at full pass 2.98 ms per 600 M rows, 1.57 ms without those global atomics. The batch
+// kernel, whose instances' keys are uniform, keeps that form: see CubeTableT.) Rows
 // outside the tables' fast domain
 // (discount > 10, tax > 8 or price >= 2^24; TPC-H data has none) take the global path, so every
 // result is exact over the whole compressed domain.
